@@ -1,0 +1,99 @@
+/*
+ * tcuscan.h -- C ABI of the B200 (sm_100a) tcuscan scan family.
+ *
+ * Plain pointers and sizes only: no torch types cross this boundary.  Every
+ * device pointer must be 16-byte aligned; every call is asynchronous on the
+ * given stream (a cudaStream_t passed as void*, NULL = legacy default stream)
+ * and returns a status code.  Kernels that need a decoupled look-back take a
+ * workspace from tcu_workspace_bytes()/tcu_workspace_init(); a workspace must
+ * not be shared by launches that can overlap on the GPU.  Device-side errors
+ * (a bounded wait that ran out) are recorded in the workspace and read back
+ * with tcu_workspace_error().
+ *
+ * Each entry point names the reference interface it replaces (path:line in
+ * huawei-csl/pytorch-tcuscan).
+ */
+#ifndef TCUSCAN_H_
+#define TCUSCAN_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define TCU_API __attribute__((visibility("default")))
+#else
+#define TCU_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum tcu_status {
+  TCU_OK = 0,
+  TCU_ERR_ARG = 1,        /* bad size / S / shape argument */
+  TCU_ERR_DTYPE = 2,      /* unsupported dtype combination */
+  TCU_ERR_LAUNCH = 3,     /* CUDA launch or API error */
+  TCU_ERR_TIMEOUT = 4,    /* a device-side bounded wait ran out */
+  TCU_ERR_OOM = 5,        /* allocation failed / budget exceeded */
+  TCU_ERR_ALIGN = 6,      /* pointer not 16-byte aligned */
+  TCU_ERR_DEVICE = 7,     /* no sm_100 device / driver entry point missing */
+  TCU_ERR_WORKSPACE = 8   /* workspace missing or too small */
+} tcu_status_t;
+
+typedef enum tcu_dtype {
+  TCU_INT8 = 1,
+  TCU_INT16 = 2,
+  TCU_INT32 = 3,
+  TCU_INT64 = 4,
+  TCU_FLOAT16 = 5,
+  TCU_BFLOAT16 = 6,
+  TCU_FLOAT32 = 7,
+  TCU_FLOAT64 = 8,
+  TCU_UINT32 = 9
+} tcu_dtype_t;
+
+/* ---- library / workspace ------------------------------------------------ */
+TCU_API int tcu_version(void);
+TCU_API const char* tcu_status_string(int status);
+/* Message of the last CUDA error seen by this thread (empty if none). */
+TCU_API const char* tcu_last_error_message(void);
+/* Timeout of every device-side bounded wait, in nanoseconds (default 4 s). */
+TCU_API void tcu_set_timeout_ns(uint64_t ns);
+TCU_API uint64_t tcu_get_timeout_ns(void);
+/* Bytes of workspace needed by the look-back kernels for n elements at tile
+ * parameter S (covers every entry point below for that n and S). */
+TCU_API size_t tcu_workspace_bytes(int64_t n, int S);
+/* Zero a freshly allocated workspace (once; later launches self-reset it). */
+TCU_API tcu_status_t tcu_workspace_init(void* ws, size_t ws_bytes, void* stream);
+/* Synchronise `stream`, copy out the sticky device error of a workspace:
+ * info[0] = status code, info[1] = site, info[2] = chunk.  clear != 0 resets
+ * it.  Returns info[0]. */
+TCU_API tcu_status_t tcu_workspace_error(void* ws, uint32_t info[3], int clear, void* stream);
+
+/* ---- scans ---------------------------------------------------------------
+ * Inclusive prefix sum z = cumsum(x) + start.  x: int8 -> z int32 (exact,
+ * two's-complement wrap like torch.cumsum(dtype=int32)); x: fp16 -> z fp32
+ * (FP32 tensor-core rows, FP64 carry chain).  S in {16,32,64,128} is the row
+ * length of the S x S triangular tile multiplied on the tensor cores.
+ * Replaces run_scan_multi_core (src/torch/torch_scan.h:184-241),
+ * run_scan_multi_core_no_l2 (:253-304), run_scan_single_core (:47-110,
+ * start = starting_sum) and run_scan_multi_cube (:416-466).              */
+TCU_API tcu_status_t tcu_scan(const void* x, tcu_dtype_t x_dtype, int64_t n, int S, double start, void* z, void* ws,
+                      size_t ws_bytes, void* stream);
+
+/* Per-row scans of n_rows rows of S elements (z has n_rows*S elements).
+ * Replaces run_row_scan (src/torch/torch_scan.h:312-351).                 */
+TCU_API tcu_status_t tcu_row_scan(const void* x, tcu_dtype_t x_dtype, int64_t n_rows, int S, void* z, void* ws,
+                          size_t ws_bytes, void* stream);
+
+/* Scan of every consecutive S*S block (n must be a multiple of S*S).
+ * Replaces run_block_scan (src/torch/torch_scan.h:362-405).               */
+TCU_API tcu_status_t tcu_block_scan(const void* x, tcu_dtype_t x_dtype, int64_t n, int S, void* z, void* ws,
+                            size_t ws_bytes, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TCUSCAN_H_ */

@@ -1,0 +1,261 @@
+// tcu_capi.cu -- extern "C" entry points of libtcuscan.so: argument checks,
+// TMA tensor-map construction, kernel selection and launch.
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <cudaTypedefs.h>
+
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+
+#include "tcu_host.h"
+#include "tcu_scan_tc.cuh"
+
+namespace tcu {
+
+static thread_local char g_errmsg[512] = "";
+static uint64_t g_timeout_ns = 4000000000ull;
+
+tcu_status_t cuda_fail(cudaError_t e, const char* what) {
+  snprintf(g_errmsg, sizeof(g_errmsg), "%s: %s", what, cudaGetErrorString(e));
+  return TCU_ERR_LAUNCH;
+}
+
+uint64_t timeout_ns() { return g_timeout_ns; }
+
+int sm_count() {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  static int cached[64] = {0};
+  if (dev < 0 || dev >= 64) return 148;
+  if (!cached[dev]) {
+    int v = 0;
+    cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+    cached[dev] = v > 0 ? v : 148;
+  }
+  return cached[dev];
+}
+
+static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  return fn;
+}
+
+// 2-D row-major tensor [rows, cols] of `elem`-byte elements, box [box_rows,
+// box_cols], swizzle span = box_cols * elem bytes (32/64/128).
+tcu_status_t make_map_2d(CUtensorMap* m, const void* base, CUtensorMapDataType dt, int elem, uint64_t cols,
+                         uint64_t rows, uint32_t box_cols, uint32_t box_rows) {
+  auto fn = encode_fn();
+  if (!fn) {
+    snprintf(g_errmsg, sizeof(g_errmsg), "cuTensorMapEncodeTiled entry point unavailable");
+    return TCU_ERR_DEVICE;
+  }
+  const uint32_t span = box_cols * elem;
+  CUtensorMapSwizzle sw = span == 128 ? CU_TENSOR_MAP_SWIZZLE_128B
+                                      : (span == 64 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B);
+  cuuint64_t dims[2] = {cols, rows};
+  cuuint64_t strides[1] = {cols * (uint64_t)elem};
+  cuuint32_t box[2] = {box_cols, box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = fn(m, dt, 2, const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, sw,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    snprintf(g_errmsg, sizeof(g_errmsg), "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return TCU_ERR_LAUNCH;
+  }
+  return TCU_OK;
+}
+
+bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+// Workspace layout: header | flags[cap] | vals[cap] (cap from the byte size).
+int64_t ws_capacity(size_t bytes) {
+  if (bytes < 256) return 0;
+  return (int64_t)((bytes - 256) / (sizeof(uint32_t) + sizeof(LbValue)));
+}
+void ws_pointers(void* ws, size_t bytes, uint32_t** flags, LbValue** vals) {
+  const int64_t cap = ws_capacity(bytes);
+  uint8_t* b = static_cast<uint8_t*>(ws);
+  *flags = reinterpret_cast<uint32_t*>(b + sizeof(WsHeader));
+  size_t vo = sizeof(WsHeader) + (size_t)cap * sizeof(uint32_t);
+  vo = (vo + 63) & ~(size_t)63;
+  *vals = reinterpret_cast<LbValue*>(b + vo);
+}
+
+// ---------------------------------------------------------------------------
+// Tensor-core scan launcher.
+template <typename InT, int W, int MODE>
+static tcu_status_t launch_scan_tc(const void* x, int64_t n, void* z, double start_f, long long start_i,
+                                   int seg_rows, void* ws, size_t ws_bytes, cudaStream_t st) {
+  using C = ScanCfg<InT, W>;
+  ScanParams p{};
+  p.x = x;
+  p.z = z;
+  p.n = n;
+  p.full_rows = n / W;
+  p.tail = (int32_t)(n % W);
+  p.seg_rows = seg_rows;
+  const int64_t total_rows = p.full_rows + (p.tail ? 1 : 0);
+  p.num_chunks = (total_rows + 127) / 128;
+  p.start_f = start_f;
+  p.start_i = start_i;
+  p.timeout_ns = g_timeout_ns;
+  if (ws == nullptr || ws_capacity(ws_bytes) < p.num_chunks) {
+    snprintf(g_errmsg, sizeof(g_errmsg), "workspace too small: %lld chunks need %zu bytes",
+             (long long)p.num_chunks, tcu_workspace_bytes(n, W));
+    return TCU_ERR_WORKSPACE;
+  }
+  p.ws = static_cast<WsHeader*>(ws);
+  ws_pointers(ws, ws_bytes, &p.flags, &p.vals);
+
+  CUtensorMap in_map, out_map;
+  std::memset(&in_map, 0, sizeof(in_map));
+  std::memset(&out_map, 0, sizeof(out_map));
+  p.has_in_map = p.full_rows > 0;
+  p.has_out_map = p.full_rows > 0;
+  if (p.full_rows > 0) {
+    const CUtensorMapDataType idt = C::IS_INT ? CU_TENSOR_MAP_DATA_TYPE_UINT8
+                                              : (sizeof(InT) == 2 ? CU_TENSOR_MAP_DATA_TYPE_UINT16
+                                                                  : CU_TENSOR_MAP_DATA_TYPE_UINT32);
+    tcu_status_t s = make_map_2d(&in_map, x, idt, C::ELEM, W, (uint64_t)p.full_rows, C::SW / C::ELEM, 128);
+    if (s != TCU_OK) return s;
+    s = make_map_2d(&out_map, z, CU_TENSOR_MAP_DATA_TYPE_UINT32, 4, W, (uint64_t)p.full_rows, C::OBW, 128);
+    if (s != TCU_OK) return s;
+  }
+  const int smem = C::SMEM_BYTES < 120 * 1024 ? 120 * 1024 : C::SMEM_BYTES;
+  auto kern = scan_tc_kernel<InT, W, MODE>;
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
+    attr_set = true;
+  }
+  int grid = sm_count();
+  if (p.num_chunks < grid) grid = (int)p.num_chunks;
+  kern<<<grid, kThreads, smem, st>>>(in_map, out_map, p);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "scan_tc_kernel launch");
+  return TCU_OK;
+}
+
+template <int MODE>
+static tcu_status_t dispatch_scan(const void* x, tcu_dtype_t dt, int64_t n, int S, void* z, double start, int seg_rows,
+                                  void* ws, size_t ws_bytes, cudaStream_t st) {
+  const long long si = (long long)start;
+  if (dt == TCU_INT8) {
+    switch (S) {
+      case 32: return launch_scan_tc<int8_t, 32, MODE>(x, n, z, 0.0, si, seg_rows, ws, ws_bytes, st);
+      case 64: return launch_scan_tc<int8_t, 64, MODE>(x, n, z, 0.0, si, seg_rows, ws, ws_bytes, st);
+      case 128: return launch_scan_tc<int8_t, 128, MODE>(x, n, z, 0.0, si, seg_rows, ws, ws_bytes, st);
+      default: return TCU_ERR_ARG;
+    }
+  }
+  if (dt == TCU_FLOAT16) {
+    switch (S) {
+      case 16: return launch_scan_tc<__half, 16, MODE>(x, n, z, start, 0, seg_rows, ws, ws_bytes, st);
+      case 32: return launch_scan_tc<__half, 32, MODE>(x, n, z, start, 0, seg_rows, ws, ws_bytes, st);
+      case 64: return launch_scan_tc<__half, 64, MODE>(x, n, z, start, 0, seg_rows, ws, ws_bytes, st);
+      case 128: return launch_scan_tc<__half, 128, MODE>(x, n, z, start, 0, seg_rows, ws, ws_bytes, st);
+      default: return TCU_ERR_ARG;
+    }
+  }
+  return TCU_ERR_DTYPE;
+}
+
+}  // namespace tcu
+
+using namespace tcu;
+
+extern "C" {
+
+int tcu_version(void) { return 100; }
+
+const char* tcu_status_string(int s) {
+  switch (s) {
+    case TCU_OK: return "ok";
+    case TCU_ERR_ARG: return "invalid argument";
+    case TCU_ERR_DTYPE: return "unsupported dtype";
+    case TCU_ERR_LAUNCH: return "CUDA launch error";
+    case TCU_ERR_TIMEOUT: return "device wait timed out";
+    case TCU_ERR_OOM: return "out of memory";
+    case TCU_ERR_ALIGN: return "pointer not 16-byte aligned";
+    case TCU_ERR_DEVICE: return "device unsupported";
+    case TCU_ERR_WORKSPACE: return "workspace missing or too small";
+    default: return "unknown status";
+  }
+}
+
+const char* tcu_last_error_message(void) { return g_errmsg; }
+
+void tcu_set_timeout_ns(uint64_t ns) { g_timeout_ns = ns ? ns : 4000000000ull; }
+uint64_t tcu_get_timeout_ns(void) { return g_timeout_ns; }
+
+size_t tcu_workspace_bytes(int64_t n, int S) {
+  if (S < 16) S = 16;
+  const int64_t rows = (n + S - 1) / S;
+  int64_t chunks = (rows + 127) / 128;
+  if (chunks < 1) chunks = 1;
+  return 256 + (size_t)chunks * (sizeof(uint32_t) + sizeof(LbValue)) + 64;
+}
+
+tcu_status_t tcu_workspace_init(void* ws, size_t ws_bytes, void* stream) {
+  if (!ws || ws_bytes < 256) return TCU_ERR_WORKSPACE;
+  cudaError_t e = cudaMemsetAsync(ws, 0, ws_bytes, (cudaStream_t)stream);
+  return e == cudaSuccess ? TCU_OK : cuda_fail(e, "cudaMemsetAsync(workspace)");
+}
+
+tcu_status_t tcu_workspace_error(void* ws, uint32_t info[3], int clear, void* stream) {
+  if (!ws) return TCU_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  WsHeader h;
+  cudaError_t e = cudaMemcpyAsync(&h, ws, sizeof(h), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_fail(e, "read workspace error");
+  info[0] = h.error;
+  info[1] = h.err_site;
+  info[2] = h.err_chunk;
+  if (clear && h.error) {
+    e = cudaMemsetAsync(&static_cast<WsHeader*>(ws)->error, 0, 3 * sizeof(uint32_t), st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_fail(e, "clear workspace error");
+  }
+  return (tcu_status_t)h.error;
+}
+
+tcu_status_t tcu_scan(const void* x, tcu_dtype_t x_dtype, int64_t n, int S, double start, void* z, void* ws,
+                      size_t ws_bytes, void* stream) {
+  if (n < 0) return TCU_ERR_ARG;
+  if (n == 0) return TCU_OK;
+  if (!x || !z) return TCU_ERR_ARG;
+  if (!aligned16(x) || !aligned16(z)) return TCU_ERR_ALIGN;
+  if (x_dtype == TCU_INT8 && S == 16) S = 32;  // full scans are independent of S; 8-bit K step is 32
+  return dispatch_scan<kScanFull>(x, x_dtype, n, S, z, start, 0, ws, ws_bytes, (cudaStream_t)stream);
+}
+
+tcu_status_t tcu_row_scan(const void* x, tcu_dtype_t x_dtype, int64_t n_rows, int S, void* z, void* ws,
+                          size_t ws_bytes, void* stream) {
+  if (n_rows < 0) return TCU_ERR_ARG;
+  if (n_rows == 0) return TCU_OK;
+  if (!x || !z) return TCU_ERR_ARG;
+  if (!aligned16(x) || !aligned16(z)) return TCU_ERR_ALIGN;
+  return dispatch_scan<kScanRows>(x, x_dtype, n_rows * S, S, z, 0.0, 0, ws, ws_bytes, (cudaStream_t)stream);
+}
+
+tcu_status_t tcu_block_scan(const void* x, tcu_dtype_t x_dtype, int64_t n, int S, void* z, void* ws,
+                            size_t ws_bytes, void* stream) {
+  if (n < 0 || S <= 0 || n % ((int64_t)S * S) != 0) return TCU_ERR_ARG;
+  if (n == 0) return TCU_OK;
+  if (!x || !z) return TCU_ERR_ARG;
+  if (!aligned16(x) || !aligned16(z)) return TCU_ERR_ALIGN;
+  return dispatch_scan<kScanBlocks>(x, x_dtype, n, S, z, 0.0, S, ws, ws_bytes, (cudaStream_t)stream);
+}
+
+}  // extern "C"

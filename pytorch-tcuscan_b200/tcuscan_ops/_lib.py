@@ -1,0 +1,151 @@
+"""ctypes binding of libtcuscan.so (the C ABI in include/tcuscan.h).
+
+The shared library is the product: this module only declares its signatures,
+owns the per-(device, stream) look-back workspaces, and turns non-OK status
+codes into Python exceptions.  There is no CPU fallback: importing
+tcuscan_ops without the built library raises ImportError.
+"""
+import ctypes
+import os
+import threading
+
+import torch
+
+PKG = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.environ.get("TCUSCAN_LIB", os.path.join(PKG, "lib", "libtcuscan.so"))
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(
+        f"libtcuscan.so not found at {LIB_PATH}; build it with `python pytorch-tcuscan_b200/build.py`"
+    )
+lib = ctypes.CDLL(LIB_PATH)
+
+# status codes (include/tcuscan.h)
+TCU_OK, TCU_ERR_ARG, TCU_ERR_DTYPE, TCU_ERR_LAUNCH, TCU_ERR_TIMEOUT = 0, 1, 2, 3, 4
+TCU_ERR_OOM, TCU_ERR_ALIGN, TCU_ERR_DEVICE, TCU_ERR_WORKSPACE = 5, 6, 7, 8
+
+# dtype codes
+TCU_INT8, TCU_INT16, TCU_INT32, TCU_INT64 = 1, 2, 3, 4
+TCU_FLOAT16, TCU_BFLOAT16, TCU_FLOAT32, TCU_FLOAT64, TCU_UINT32 = 5, 6, 7, 8, 9
+
+DTYPE_CODE = {
+    torch.int8: TCU_INT8,
+    torch.int16: TCU_INT16,
+    torch.int32: TCU_INT32,
+    torch.int64: TCU_INT64,
+    torch.float16: TCU_FLOAT16,
+    torch.bfloat16: TCU_BFLOAT16,
+    torch.float32: TCU_FLOAT32,
+    torch.float64: TCU_FLOAT64,
+}
+if hasattr(torch, "uint32"):
+    DTYPE_CODE[torch.uint32] = TCU_UINT32
+
+_P, _I, _I64, _U64, _SZ, _D = ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_uint64, ctypes.c_size_t, ctypes.c_double
+_ST = ctypes.c_int
+
+
+def _sig(name, restype, *argtypes):
+    f = getattr(lib, name)
+    f.restype = restype
+    f.argtypes = list(argtypes)
+    return f
+
+
+_sig("tcu_version", _I)
+_sig("tcu_status_string", ctypes.c_char_p, _I)
+_sig("tcu_last_error_message", ctypes.c_char_p)
+_sig("tcu_set_timeout_ns", None, _U64)
+_sig("tcu_get_timeout_ns", _U64)
+_sig("tcu_workspace_bytes", _SZ, _I64, _I)
+_sig("tcu_workspace_init", _ST, _P, _SZ, _P)
+_sig("tcu_workspace_error", _ST, _P, ctypes.POINTER(ctypes.c_uint32), _I, _P)
+_sig("tcu_scan", _ST, _P, _I, _I64, _I, _D, _P, _P, _SZ, _P)
+_sig("tcu_row_scan", _ST, _P, _I, _I64, _I, _P, _P, _SZ, _P)
+_sig("tcu_block_scan", _ST, _P, _I, _I64, _I, _P, _P, _SZ, _P)
+
+
+class TcuError(RuntimeError):
+    """A libtcuscan call or a device-side bounded wait failed."""
+
+    def __init__(self, status, where, detail=""):
+        self.status = int(status)
+        msg = lib.tcu_status_string(int(status)).decode()
+        last = lib.tcu_last_error_message().decode()
+        super().__init__(f"{where}: {msg}" + (f" ({detail})" if detail else "") + (f" [{last}]" if last else ""))
+
+
+def check(status, where):
+    if status != TCU_OK:
+        if status in (TCU_ERR_ARG, TCU_ERR_DTYPE, TCU_ERR_ALIGN):
+            raise ValueError(f"{where}: {lib.tcu_status_string(int(status)).decode()} "
+                             f"[{lib.tcu_last_error_message().decode()}]")
+        raise TcuError(status, where)
+
+
+def stream_ptr(device):
+    return ctypes.c_void_p(torch.cuda.current_stream(device).cuda_stream)
+
+
+class _Workspace:
+    __slots__ = ("buf", "bytes")
+
+    def __init__(self):
+        self.buf = None
+        self.bytes = 0
+
+
+_ws_lock = threading.Lock()
+_workspaces = {}
+
+SYNC_CHECK = os.environ.get("TCU_SYNC_CHECK", "0") == "1"
+
+
+def workspace(device, need_bytes):
+    """Return (ptr, bytes) of the look-back workspace of (device, current stream).
+
+    One workspace per stream keeps launches that may overlap on the GPU from
+    sharing look-back state; launches on one stream are ordered, and each one
+    leaves the workspace reset for the next (epoch-tagged flags)."""
+    dev = torch.device(device)
+    stream = torch.cuda.current_stream(dev)
+    key = (dev.index, stream.cuda_stream)
+    with _ws_lock:
+        ws = _workspaces.get(key)
+        if ws is None:
+            ws = _workspaces[key] = _Workspace()
+        if ws.bytes < need_bytes:
+            nbytes = max(int(need_bytes), 1 << 20, 2 * ws.bytes)
+            ws.buf = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+            ws.bytes = nbytes
+            check(lib.tcu_workspace_init(ctypes.c_void_p(ws.buf.data_ptr()), _SZ(nbytes),
+                                         ctypes.c_void_p(stream.cuda_stream)), "tcu_workspace_init")
+        return ctypes.c_void_p(ws.buf.data_ptr()), _SZ(ws.bytes)
+
+
+def workspace_error(device=None, clear=True):
+    """Synchronise and return (code, site, chunk) of the current stream's workspace."""
+    dev = torch.device(device if device is not None else torch.cuda.current_device())
+    if dev.type == "cuda" and dev.index is None:
+        dev = torch.device("cuda", torch.cuda.current_device())
+    stream = torch.cuda.current_stream(dev)
+    ws = _workspaces.get((dev.index, stream.cuda_stream))
+    if ws is None or ws.buf is None:
+        return (0, 0, 0)
+    info = (ctypes.c_uint32 * 3)()
+    lib.tcu_workspace_error(ctypes.c_void_p(ws.buf.data_ptr()), info, int(clear), ctypes.c_void_p(stream.cuda_stream))
+    return (int(info[0]), int(info[1]), int(info[2]))
+
+
+def raise_device_error(device=None):
+    code, site, chunk = workspace_error(device, clear=True)
+    if code != TCU_OK:
+        raise TcuError(code, "device", f"site {site}, chunk {chunk}")
+
+
+def set_timeout_ns(ns):
+    lib.tcu_set_timeout_ns(_U64(int(ns)))
+
+
+def get_timeout_ns():
+    return int(lib.tcu_get_timeout_ns())

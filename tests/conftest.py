@@ -19,3 +19,35 @@ def golden():
     import numpy as np
 
     return np.load(os.path.join(REPO, "tests", "golden", "golden.npz"))
+
+
+def _ensure_lib():
+    """Build libtcuscan.so in-tree when it is missing (nvcc cross-compiles on CPU)."""
+    lib = os.path.join(PKG, "lib", "libtcuscan.so")
+    if not os.path.exists(lib):
+        sys.path.insert(0, PKG)
+        import build as _b
+
+        _b.build()
+    return lib
+
+
+LIB_PATH = _ensure_lib()
+
+
+def cuda_ok():
+    try:
+        import torch
+
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+def pytest_collection_modifyitems(config, items):
+    if cuda_ok():
+        return
+    skip = pytest.mark.skip(reason="no CUDA device")
+    for it in items:
+        if "gpu" in it.keywords:
+            it.add_marker(skip)

@@ -1,0 +1,88 @@
+"""C-ABI checks that need no GPU: the library loads, exports every symbol that
+include/*.h declares, and rejects bad arguments before touching the device."""
+import ctypes
+import glob
+import os
+import re
+
+import pytest
+import torch
+
+from conftest import LIB_PATH, REPO
+
+HEADERS = sorted(glob.glob(os.path.join(REPO, "include", "*.h")))
+
+
+def _declared():
+    names = []
+    for h in HEADERS:
+        txt = open(h).read()
+        names += re.findall(r"TCU_API\s+[\w\s\*]+?\b(tcu_\w+)\s*\(", txt)
+    return sorted(set(names))
+
+
+def test_headers_exist():
+    assert HEADERS, "include/*.h missing"
+    assert len(_declared()) >= 8
+
+
+def test_library_exports_every_declared_symbol():
+    lib = ctypes.CDLL(LIB_PATH)
+    missing = [n for n in _declared() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_status_strings_and_version():
+    import tcuscan_ops._lib as L
+
+    assert L.lib.tcu_version() >= 100
+    for code in range(0, 9):
+        assert L.lib.tcu_status_string(code)
+    assert L.lib.tcu_status_string(999) == b"unknown status"
+
+
+def test_workspace_bytes_monotone():
+    import tcuscan_ops._lib as L
+
+    prev = 0
+    for n in (1, 1000, 1 << 20, 1 << 28):
+        b = L.lib.tcu_workspace_bytes(n, 64)
+        assert b >= prev and b >= 256
+        prev = b
+    assert L.lib.tcu_workspace_bytes(1 << 28, 16) > L.lib.tcu_workspace_bytes(1 << 28, 128)
+
+
+def test_argument_errors_before_device():
+    import tcuscan_ops._lib as L
+
+    # n == 0 is a no-op; negative n, unaligned pointers, bad S are rejected on the host
+    assert L.lib.tcu_scan(None, L.TCU_INT8, 0, 64, 0.0, None, None, 0, None) == L.TCU_OK
+    assert L.lib.tcu_scan(None, L.TCU_INT8, -1, 64, 0.0, None, None, 0, None) == L.TCU_ERR_ARG
+    assert L.lib.tcu_scan(ctypes.c_void_p(0x1001), L.TCU_INT8, 10, 64, 0.0, ctypes.c_void_p(0x2000), None, 0,
+                          None) == L.TCU_ERR_ALIGN
+    assert L.lib.tcu_block_scan(ctypes.c_void_p(0x1000), L.TCU_FLOAT16, 100, 16, ctypes.c_void_p(0x2000), None, 0,
+                                None) == L.TCU_ERR_ARG
+
+
+def test_python_layer_rejects_cpu_tensors():
+    import tcuscan_ops
+
+    with pytest.raises(ValueError):
+        tcuscan_ops.run_scan_multi_core(torch.zeros(10, dtype=torch.int8), 64)
+    with pytest.raises(ValueError):
+        tcuscan_ops.run_scan_multi_core(torch.zeros(10, dtype=torch.int8, device="meta"), 64)
+
+
+def test_run_scan_cpu_api():
+    import tcuscan_ops
+
+    x = torch.randint(0, 10, (1000,), dtype=torch.int8)
+    assert torch.equal(tcuscan_ops.run_scan_cpu(x), torch.cumsum(x, 0, dtype=torch.int32))
+    xf = torch.randn(1000).half()
+    assert tcuscan_ops.run_scan_cpu(xf).dtype == torch.float32
+
+
+def test_tcuscan_package_reexports():
+    import tcuscan
+
+    assert hasattr(tcuscan, "run_scan_multi_core") and hasattr(tcuscan, "run_row_scan")
