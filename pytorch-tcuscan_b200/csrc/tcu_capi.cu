@@ -76,19 +76,12 @@ tcu_status_t make_map_2d(CUtensorMap* m, const void* base, CUtensorMapDataType d
 
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
-// Workspace layout: header | flags[cap] | vals[cap] (cap from the byte size).
+// Workspace layout: 64-byte header | 64 bytes pad | TileDesc[cap].
 int64_t ws_capacity(size_t bytes) {
   if (bytes < 256) return 0;
-  return (int64_t)((bytes - 256) / (sizeof(uint32_t) + sizeof(LbValue)));
+  return (int64_t)((bytes - 128) / sizeof(TileDesc));
 }
-void ws_pointers(void* ws, size_t bytes, uint32_t** flags, LbValue** vals) {
-  const int64_t cap = ws_capacity(bytes);
-  uint8_t* b = static_cast<uint8_t*>(ws);
-  *flags = reinterpret_cast<uint32_t*>(b + sizeof(WsHeader));
-  size_t vo = sizeof(WsHeader) + (size_t)cap * sizeof(uint32_t);
-  vo = (vo + 63) & ~(size_t)63;
-  *vals = reinterpret_cast<LbValue*>(b + vo);
-}
+TileDesc* ws_descs(void* ws) { return reinterpret_cast<TileDesc*>(static_cast<uint8_t*>(ws) + 128); }
 
 // ---------------------------------------------------------------------------
 // Tensor-core scan launcher.
@@ -104,27 +97,26 @@ static tcu_status_t launch_scan_tc(const void* x, int64_t n, void* z, double sta
   p.tail = (int32_t)(n % W);
   p.seg_rows = seg_rows;
   const int64_t total_rows = p.full_rows + (p.tail ? 1 : 0);
-  p.num_chunks = (total_rows + 127) / 128;
+  const int64_t tile_rows = 128 * C::BPT;
+  p.num_tiles = (total_rows + tile_rows - 1) / tile_rows;
   p.start_f = start_f;
   p.start_i = start_i;
   p.timeout_ns = g_timeout_ns;
-  if (ws == nullptr || ws_capacity(ws_bytes) < p.num_chunks) {
-    snprintf(g_errmsg, sizeof(g_errmsg), "workspace too small: %lld chunks need %zu bytes",
-             (long long)p.num_chunks, tcu_workspace_bytes(n, W));
+  if (ws == nullptr || ws_capacity(ws_bytes) < p.num_tiles) {
+    snprintf(g_errmsg, sizeof(g_errmsg), "workspace too small: %lld tiles need %zu bytes", (long long)p.num_tiles,
+             tcu_workspace_bytes(n, W));
     return TCU_ERR_WORKSPACE;
   }
+  if (p.num_tiles > 0xFFFFFFF0ll) return TCU_ERR_ARG;
   p.ws = static_cast<WsHeader*>(ws);
-  ws_pointers(ws, ws_bytes, &p.flags, &p.vals);
+  p.descs = ws_descs(ws);
 
   CUtensorMap in_map, out_map;
   std::memset(&in_map, 0, sizeof(in_map));
   std::memset(&out_map, 0, sizeof(out_map));
-  p.has_in_map = p.full_rows > 0;
-  p.has_out_map = p.full_rows > 0;
+  p.has_map = p.full_rows > 0;
   if (p.full_rows > 0) {
-    const CUtensorMapDataType idt = C::IS_INT ? CU_TENSOR_MAP_DATA_TYPE_UINT8
-                                              : (sizeof(InT) == 2 ? CU_TENSOR_MAP_DATA_TYPE_UINT16
-                                                                  : CU_TENSOR_MAP_DATA_TYPE_UINT32);
+    const CUtensorMapDataType idt = C::IS_INT ? CU_TENSOR_MAP_DATA_TYPE_UINT8 : CU_TENSOR_MAP_DATA_TYPE_UINT16;
     tcu_status_t s = make_map_2d(&in_map, x, idt, C::ELEM, W, (uint64_t)p.full_rows, C::SW / C::ELEM, 128);
     if (s != TCU_OK) return s;
     s = make_map_2d(&out_map, z, CU_TENSOR_MAP_DATA_TYPE_UINT32, 4, W, (uint64_t)p.full_rows, C::OBW, 128);
@@ -139,7 +131,7 @@ static tcu_status_t launch_scan_tc(const void* x, int64_t n, void* z, double sta
     attr_set = true;
   }
   int grid = sm_count();
-  if (p.num_chunks < grid) grid = (int)p.num_chunks;
+  if (p.num_tiles < grid) grid = (int)p.num_tiles;
   kern<<<grid, kThreads, smem, st>>>(in_map, out_map, p);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "scan_tc_kernel launch");
@@ -199,11 +191,10 @@ void tcu_set_timeout_ns(uint64_t ns) { g_timeout_ns = ns ? ns : 4000000000ull; }
 uint64_t tcu_get_timeout_ns(void) { return g_timeout_ns; }
 
 size_t tcu_workspace_bytes(int64_t n, int S) {
-  if (S < 16) S = 16;
-  const int64_t rows = (n + S - 1) / S;
-  int64_t chunks = (rows + 127) / 128;
-  if (chunks < 1) chunks = 1;
-  return 256 + (size_t)chunks * (sizeof(uint32_t) + sizeof(LbValue)) + 64;
+  (void)S;  // a tile is 32768 elements for every S
+  if (n < 0) n = 0;
+  const int64_t tiles = (n + 32767) / 32768 + 2;
+  return 128 + (size_t)tiles * sizeof(TileDesc);
 }
 
 tcu_status_t tcu_workspace_init(void* ws, size_t ws_bytes, void* stream) {

@@ -19,38 +19,23 @@ namespace tcu {
 // ---------------------------------------------------------------------------
 // Workspace header shared by every look-back kernel launch.  The tile
 // counter and done counter are reset by the last CTA of each launch, and the
-// epoch is bumped, so the per-chunk flags of earlier launches read as stale
-// without any memset between launches (CUDA-graph safe).
+// epoch is bumped, so the per-tile descriptors of earlier launches read as
+// stale without any memset between launches (CUDA-graph safe).
 struct WsHeader {
-  uint32_t chunk_counter;  // dynamic chunk assignment (atomicAdd)
+  uint32_t tile_counter;   // dynamic tile assignment (atomicAdd)
   uint32_t done_ctas;      // CTAs finished in this launch
-  uint32_t epoch;          // launch generation, tags the per-chunk flags
+  uint32_t epoch;          // launch generation, tags the tile descriptors
   uint32_t error;          // first error code (sticky until read by the host)
   uint32_t err_site;       // where it happened (kernel-defined)
-  uint32_t err_chunk;      // chunk being processed
+  uint32_t err_chunk;      // tile being processed
   uint32_t pad[10];
 };
 static_assert(sizeof(WsHeader) == 64, "header size");
 
-// Per-chunk look-back record.  Flag word: bits[1:0] state, bit 2 = the chunk
-// contains a segment start (its aggregate is already a complete carry),
-// bits[31:3] = epoch.
+// Look-back descriptor states: bits[1:0] state, bit 2 = the tile contains a
+// segment start (its aggregate is already a complete carry), bits[31:3] =
+// launch epoch.
 enum : uint32_t { LB_INVALID = 0, LB_AGG = 1, LB_INC = 2, LB_SEGSTART = 4 };
-struct LbValue {
-  double agg_f;   // floating aggregate (FP64 carry chain)
-  double inc_f;   // floating inclusive prefix
-  long long agg_i;  // integer aggregate
-  long long inc_i;  // integer inclusive prefix
-};
-
-__host__ __device__ inline size_t ws_flags_offset() { return sizeof(WsHeader); }
-__host__ __device__ inline size_t ws_vals_offset(int64_t max_chunks) {
-  size_t o = sizeof(WsHeader) + (size_t)max_chunks * sizeof(uint32_t);
-  return (o + 63) & ~(size_t)63;
-}
-__host__ __device__ inline size_t ws_bytes_for(int64_t max_chunks) {
-  return ws_vals_offset(max_chunks) + (size_t)max_chunks * sizeof(LbValue) + 64;
-}
 
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ uint64_t globaltimer() {
@@ -249,6 +234,23 @@ enum : uint32_t { CF_F32 = 1, CF_S32 = 2, AB_F16 = 0, AB_BF16 = 1, AB_S8 = 1 };
 __device__ __forceinline__ uint32_t swz(uint32_t o, uint32_t span) {
   const uint32_t mask = span == 128 ? 0x70u : (span == 64 ? 0x30u : 0x10u);
   return o ^ ((o >> 3) & mask);
+}
+
+// ---------------------------------------------------------------------------
+// Warp helpers.
+template <typename V>
+__device__ __forceinline__ V warp_sum_any(V v) {
+#pragma unroll
+  for (int d = 16; d >= 1; d >>= 1) v += __shfl_xor_sync(0xffffffffu, v, d);
+  return v;
+}
+__device__ __forceinline__ void bulk_wait_read1() { asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory"); }
+
+// 32 lanes x 32 bit, one column per thread.
+__device__ __forceinline__ uint32_t tmem_ld1(uint32_t taddr) {
+  uint32_t r;
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];" : "=r"(r) : "r"(taddr));
+  return r;
 }
 
 // ---------------------------------------------------------------------------

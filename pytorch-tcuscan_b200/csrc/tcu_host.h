@@ -4,7 +4,7 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
-#include "tcu_device.cuh"
+#include "tcu_lookback.cuh"
 #include "tcuscan.h"
 
 namespace tcu {
@@ -16,6 +16,6 @@ tcu_status_t make_map_2d(CUtensorMap* m, const void* base, CUtensorMapDataType d
                          uint64_t rows, uint32_t box_cols, uint32_t box_rows);
 bool aligned16(const void* p);
 int64_t ws_capacity(size_t bytes);
-void ws_pointers(void* ws, size_t bytes, uint32_t** flags, LbValue** vals);
+TileDesc* ws_descs(void* ws);
 
 }  // namespace tcu

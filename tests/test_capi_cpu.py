@@ -47,9 +47,11 @@ def test_workspace_bytes_monotone():
     prev = 0
     for n in (1, 1000, 1 << 20, 1 << 28):
         b = L.lib.tcu_workspace_bytes(n, 64)
-        assert b >= prev and b >= 256
+        assert b >= prev and b >= 128
         prev = b
-    assert L.lib.tcu_workspace_bytes(1 << 28, 16) > L.lib.tcu_workspace_bytes(1 << 28, 128)
+    # one 16-byte look-back descriptor per 32768-element tile, whatever S is
+    assert L.lib.tcu_workspace_bytes(1 << 28, 16) == L.lib.tcu_workspace_bytes(1 << 28, 128)
+    assert L.lib.tcu_workspace_bytes(1 << 28, 64) >= 16 * ((1 << 28) // 32768)
 
 
 def test_argument_errors_before_device():
