@@ -201,6 +201,7 @@ def main():
     ap.add_argument("--S", type=int, default=64)
     ap.add_argument("--n", type=int, default=1 << 28)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--phases", action="store_true", help="print a per-phase device-time breakdown (diagnostics)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -235,6 +236,17 @@ def main():
         step()
     torch.cuda.synchronize()
     tcuscan_ops.raise_device_error(dev)
+    if args.phases:
+        from tcuscan_ops import _lib as L
+
+        L.phase_times(dev, clear=True)
+        L.set_phase_profile(True)
+        for _ in range(10):
+            step()
+        torch.cuda.synchronize()
+        L.set_phase_profile(False)
+        ph = L.phase_times(dev, clear=True)
+        print(json.dumps({"phases_ns_sum_over_10_launches": ph}), file=sys.stderr, flush=True)
 
     props = torch.cuda.get_device_properties(dev)
     bus = None

@@ -70,6 +70,13 @@ TCU_API tcu_status_t tcu_workspace_init(void* ws, size_t ws_bytes, void* stream)
  * info[0] = status code, info[1] = site, info[2] = chunk.  clear != 0 resets
  * it.  Returns info[0]. */
 TCU_API tcu_status_t tcu_workspace_error(void* ws, uint32_t info[3], int clear, void* stream);
+/* Diagnostics: when enabled, the scan kernels add per-phase device time (ns)
+ * to eight counters in the workspace: 0 epilogue wait for the MMA, 1 row
+ * totals, 2 look-back, 3 drain, 4 producer stage waits, 5 MMA data waits,
+ * 6 MMA TMEM waits, 7 tiles.  Read (and optionally clear) them with
+ * tcu_workspace_phase_ns (synchronises the stream).  Off by default. */
+TCU_API void tcu_set_phase_profile(int enable);
+TCU_API tcu_status_t tcu_workspace_phase_ns(void* ws, uint64_t out[8], int clear, void* stream);
 
 /* ---- scans ---------------------------------------------------------------
  * Inclusive prefix sum z = cumsum(x) + start.  x: int8 -> z int32 (exact,

@@ -15,6 +15,7 @@ namespace tcu {
 
 static thread_local char g_errmsg[512] = "";
 static uint64_t g_timeout_ns = 4000000000ull;
+static int g_phase_profile = 0;
 
 tcu_status_t cuda_fail(cudaError_t e, const char* what) {
   snprintf(g_errmsg, sizeof(g_errmsg), "%s: %s", what, cudaGetErrorString(e));
@@ -82,6 +83,10 @@ int64_t ws_capacity(size_t bytes) {
   return (int64_t)((bytes - 128) / sizeof(TileDesc));
 }
 TileDesc* ws_descs(void* ws) { return reinterpret_cast<TileDesc*>(static_cast<uint8_t*>(ws) + 128); }
+// Eight 64-bit phase counters live in the 64 bytes between header and descriptors.
+unsigned long long* ws_phase_counters(void* ws) {
+  return reinterpret_cast<unsigned long long*>(static_cast<uint8_t*>(ws) + 64);
+}
 
 // ---------------------------------------------------------------------------
 // Tensor-core scan launcher.
@@ -110,6 +115,7 @@ static tcu_status_t launch_scan_tc(const void* x, int64_t n, void* z, double sta
   if (p.num_tiles > 0xFFFFFFF0ll) return TCU_ERR_ARG;
   p.ws = static_cast<WsHeader*>(ws);
   p.descs = ws_descs(ws);
+  p.phase_ns = g_phase_profile ? ws_phase_counters(ws) : nullptr;
 
   CUtensorMap in_map, out_map;
   std::memset(&in_map, 0, sizeof(in_map));
@@ -186,6 +192,20 @@ const char* tcu_status_string(int s) {
 }
 
 const char* tcu_last_error_message(void) { return g_errmsg; }
+
+void tcu_set_phase_profile(int enable) { g_phase_profile = enable ? 1 : 0; }
+
+tcu_status_t tcu_workspace_phase_ns(void* ws, uint64_t out[8], int clear, void* stream) {
+  if (!ws) return TCU_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaError_t e = cudaMemcpyAsync(out, ws_phase_counters(ws), 8 * sizeof(uint64_t), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e == cudaSuccess && clear) {
+    e = cudaMemsetAsync(ws_phase_counters(ws), 0, 8 * sizeof(uint64_t), st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  }
+  return e == cudaSuccess ? TCU_OK : cuda_fail(e, "phase counters");
+}
 
 void tcu_set_timeout_ns(uint64_t ns) { g_timeout_ns = ns ? ns : 4000000000ull; }
 uint64_t tcu_get_timeout_ns(void) { return g_timeout_ns; }

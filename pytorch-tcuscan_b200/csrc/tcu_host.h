@@ -17,5 +17,6 @@ tcu_status_t make_map_2d(CUtensorMap* m, const void* base, CUtensorMapDataType d
 bool aligned16(const void* p);
 int64_t ws_capacity(size_t bytes);
 TileDesc* ws_descs(void* ws);
+unsigned long long* ws_phase_counters(void* ws);
 
 }  // namespace tcu

@@ -1,8 +1,8 @@
 // tcu_lookback.cuh -- decoupled look-back across tiles (Merrill & Garland,
 // "Single-pass Parallel Prefix Scan with Decoupled Look-back", 2016), B200
-// variant: one 16-byte descriptor per tile, a 128-thread warpgroup inspects a
-// 512-tile window per round, and the carry chain is FP64 (floating scans) or
-// int64 (integer scans).
+// variant: one 16-byte descriptor per tile, one warp inspects a 512-tile
+// window per round (16 independent loads in flight per lane), and the carry
+// chain is FP64 (floating scans) or int64 (integer scans).
 #pragma once
 
 #include "tcu_device.cuh"
@@ -40,51 +40,123 @@ __device__ __forceinline__ V v_from_bits(unsigned long long b) {
   else return (V)(long long)b;
 }
 
-// Per-warpgroup scratch for the look-back reductions (in shared memory).
-struct LbScratch {
-  double sum_f[4];
-  long long sum_i[4];
-  uint32_t dmin[4];
-};
-
+// Run by one full warp.  Publishes the tile's aggregate (agg; agg_seg = the
+// tile contains a segment start, so its aggregate is a complete carry) and
+// returns the exclusive prefix of tile `tid` (with `start` added before tile
+// 0); then publishes the tile's inclusive prefix.  Each lane inspects 16
+// predecessors per round (a 512-tile window), so one round normally reaches
+// an inclusive prefix.  Waits are bounded; on timeout the abort flag is
+// raised and the launch reports TCU_ERR_TIMEOUT.
 template <typename V>
-__device__ __forceinline__ V wg_sum(V v, LbScratch* sc, int q, int lane, uint32_t bar_id) {
-  v = warp_sum_any(v);
-  if (lane == 0) {
-    if constexpr (__is_same(V, double)) sc->sum_f[q] = v; else sc->sum_i[q] = v;
-  }
-  named_bar_sync(bar_id, 128);
-  V t;
-  if constexpr (__is_same(V, double)) t = (sc->sum_f[0] + sc->sum_f[1]) + (sc->sum_f[2] + sc->sum_f[3]);
-  else t = (sc->sum_i[0] + sc->sum_i[1]) + (sc->sum_i[2] + sc->sum_i[3]);
-  named_bar_sync(bar_id, 128);
-  return t;
+__device__ __forceinline__ void publish_aggregate(int64_t tid, V agg, int agg_seg, V start, TileDesc* descs,
+                                                  uint32_t epoch) {
+  const uint32_t tag = (epoch & 0x1FFFFFFFu) << 3;
+  const uint32_t segbit = agg_seg ? LB_SEGSTART : 0u;
+  if (tid == 0) desc_store(descs, v_bits<V>(agg_seg ? agg : start + agg), tag | segbit | LB_INC);
+  else desc_store(descs + tid, v_bits<V>(agg), tag | segbit | LB_AGG);
 }
 
-// Run by all 128 threads of one epilogue warpgroup.  Publishes the tile's
-// aggregate (agg, agg_seg = the tile contains a segment start) and returns
-// the exclusive prefix of tile `tid` (with `start` added before tile 0), then
-// publishes the tile's inclusive prefix.  Waits are bounded; on timeout the
-// abort flag is raised and the result is meaningless (the launch reports
-// TCU_ERR_TIMEOUT).
+// publish_agg = false when another warp already published the aggregate
+// with publish_aggregate() (tile 0's inclusive prefix included).
 template <typename V>
-__device__ __forceinline__ V tile_lookback(int64_t tid, V agg, int agg_seg, V start, TileDesc* descs, uint32_t epoch,
-                                           const WaitCtx& wc, LbScratch* sc, int wg_thread, uint32_t bar_id) {
-  const int lane = wg_thread & 31, q = wg_thread >> 5;
+__device__ __forceinline__ V warp_lookback(int64_t tid, V agg, int agg_seg, V start, TileDesc* descs, uint32_t epoch,
+                                           const WaitCtx& wc, bool publish_agg = true) {
+  const int lane = threadIdx.x & 31;
   const uint32_t tag = (epoch & 0x1FFFFFFFu) << 3;
   const uint32_t segbit = agg_seg ? LB_SEGSTART : 0u;
   if (tid == 0) {
-    if (wg_thread == 0) desc_store(descs, v_bits<V>(agg_seg ? agg : start + agg), tag | segbit | LB_INC);
+    if (lane == 0 && publish_agg) desc_store(descs, v_bits<V>(agg_seg ? agg : start + agg), tag | segbit | LB_INC);
     return start;
   }
-  if (wg_thread == 0) desc_store(descs + tid, v_bits<V>(agg), tag | segbit | LB_AGG);
+  if (lane == 0 && publish_agg) desc_store(descs + tid, v_bits<V>(agg), tag | segbit | LB_AGG);
+  constexpr int K = 16;
   V acc = V(0);
   int64_t base = tid - 1;
   while (true) {
-    V val[4];
+    V val[K];
+    unsigned long long vb[K];
+    uint32_t fl[K];
     uint32_t stop_d = 0xFFFFFFFFu;
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
+    for (int k = 0; k < K; ++k) {  // issue every load first
+      const int64_t idx = base - (int64_t)(lane + 32 * k);
+      if (idx >= 0) desc_load(descs + idx, vb[k], fl[k]);
+      else { vb[k] = 0; fl[k] = tag | LB_INC; }
+    }
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const uint32_t d = (uint32_t)(lane + 32 * k);
+      const int64_t idx = base - d;
+      if (idx < 0) {
+        val[k] = (idx == -1) ? start : V(0);
+        stop_d = min(stop_d, d);
+        continue;
+      }
+      uint32_t f = fl[k];
+      if ((f & ~7u) != tag || (f & 3u) == 0u) {
+        const uint64_t t0 = globaltimer();
+        uint32_t it = 0;
+        while (true) {
+          desc_load(descs + idx, vb[k], f);
+          if ((f & ~7u) == tag && (f & 3u) != 0u) break;
+          if (aborted(wc)) { f = tag | LB_INC; vb[k] = 0; break; }
+          if ((++it & 15u) == 0u && globaltimer() - t0 > wc.timeout_ns) {
+            raise_abort(wc, 100, (uint32_t)tid);
+            f = tag | LB_INC;
+            vb[k] = 0;
+            break;
+          }
+        }
+      }
+      val[k] = v_from_bits<V>(vb[k]);
+      if ((f & 3u) == LB_INC || (f & LB_SEGSTART)) stop_d = min(stop_d, d);
+    }
+    // nearest stop: an inclusive prefix, a tile holding a segment start, or
+    // the start of the input
+    const uint32_t dmin = __reduce_min_sync(0xffffffffu, stop_d);
+    V part = V(0);
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+      if ((uint32_t)(lane + 32 * k) <= dmin) part += val[k];
+    acc += warp_sum_any(part);
+    if (dmin != 0xFFFFFFFFu) break;
+    base -= 32 * K;
+  }
+  if (lane == 0) desc_store(descs + tid, v_bits<V>(agg_seg ? agg : acc + agg), tag | segbit | LB_INC);
+  return acc;
+}
+
+// Per-warpgroup scratch for the warpgroup look-back reductions.
+struct LbScratch {
+  unsigned long long sum[4];
+  uint32_t dmin[4];
+};
+
+// Warpgroup variant (128 threads, 8 predecessors per thread: a 1024-tile
+// window per round).  The tile's aggregate was already published by another
+// warp; this publishes the inclusive prefix agg_inc + exclusive prefix.
+template <typename V>
+__device__ __forceinline__ V wg_lookback(int64_t tid, V agg_inc, V start, TileDesc* descs, uint32_t epoch,
+                                         const WaitCtx& wc, LbScratch* sc, int wg_thread, uint32_t bar_id) {
+  if (tid == 0) return start;
+  const int lane = wg_thread & 31, q = wg_thread >> 5;
+  const uint32_t tag = (epoch & 0x1FFFFFFFu) << 3;
+  constexpr int K = 8;
+  V acc = V(0);
+  int64_t base = tid - 1;
+  while (true) {
+    unsigned long long vb[K];
+    uint32_t fl[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const int64_t idx = base - (int64_t)(wg_thread + 128 * k);
+      if (idx >= 0) desc_load(descs + idx, vb[k], fl[k]);
+      else { vb[k] = 0; fl[k] = tag | LB_INC; }
+    }
+    V val[K];
+    uint32_t stop_d = 0xFFFFFFFFu;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
       const uint32_t d = (uint32_t)(wg_thread + 128 * k);
       const int64_t idx = base - d;
       if (idx < 0) {
@@ -92,44 +164,43 @@ __device__ __forceinline__ V tile_lookback(int64_t tid, V agg, int agg_seg, V st
         stop_d = min(stop_d, d);
         continue;
       }
-      unsigned long long vb;
-      uint32_t f;
-      desc_load(descs + idx, vb, f);
+      uint32_t f = fl[k];
       if ((f & ~7u) != tag || (f & 3u) == 0u) {
         const uint64_t t0 = globaltimer();
         uint32_t it = 0;
         while (true) {
-          desc_load(descs + idx, vb, f);
+          desc_load(descs + idx, vb[k], f);
           if ((f & ~7u) == tag && (f & 3u) != 0u) break;
-          if (aborted(wc)) { f = tag | LB_INC; vb = 0; break; }
+          if (aborted(wc)) { f = tag | LB_INC; vb[k] = 0; break; }
           if ((++it & 15u) == 0u && globaltimer() - t0 > wc.timeout_ns) {
             raise_abort(wc, 100, (uint32_t)tid);
             f = tag | LB_INC;
-            vb = 0;
+            vb[k] = 0;
             break;
           }
         }
       }
-      val[k] = v_from_bits<V>(vb);
+      val[k] = v_from_bits<V>(vb[k]);
       if ((f & 3u) == LB_INC || (f & LB_SEGSTART)) stop_d = min(stop_d, d);
     }
-    // nearest stop (an inclusive prefix, a tile holding a segment start, or
-    // the start of the input) over the warpgroup
-    uint32_t m = __reduce_min_sync(0xffffffffu, stop_d);
-    if (lane == 0) sc->dmin[q] = m;
+    const uint32_t wmin = __reduce_min_sync(0xffffffffu, stop_d);
+    if (lane == 0) sc->dmin[q] = wmin;
     named_bar_sync(bar_id, 128);
     const uint32_t dmin = min(min(sc->dmin[0], sc->dmin[1]), min(sc->dmin[2], sc->dmin[3]));
     V part = V(0);
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const uint32_t d = (uint32_t)(wg_thread + 128 * k);
-      if (d <= dmin) part += val[k];
-    }
-    acc += wg_sum<V>(part, sc, q, lane, bar_id);
+    for (int k = 0; k < K; ++k)
+      if ((uint32_t)(wg_thread + 128 * k) <= dmin) part += val[k];
+    part = warp_sum_any(part);
+    if (lane == 0) sc->sum[q] = v_bits<V>(part);
+    named_bar_sync(bar_id, 128);
+    acc += (v_from_bits<V>(sc->sum[0]) + v_from_bits<V>(sc->sum[1])) +
+           (v_from_bits<V>(sc->sum[2]) + v_from_bits<V>(sc->sum[3]));
+    named_bar_sync(bar_id, 128);  // scratch reused by the next round
     if (dmin != 0xFFFFFFFFu) break;
-    base -= 512;
+    base -= 128 * K;
   }
-  if (wg_thread == 0) desc_store(descs + tid, v_bits<V>(agg_seg ? agg : acc + agg), tag | segbit | LB_INC);
+  if (wg_thread == 0) desc_store(descs + tid, v_bits<V>(acc + agg_inc), tag | LB_INC);
   return acc;
 }
 

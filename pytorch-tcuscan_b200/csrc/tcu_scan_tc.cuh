@@ -51,10 +51,19 @@ struct ScanParams {
   TileDesc* descs;
   uint64_t timeout_ns;
   int has_map;        // full_rows > 0: TMA maps are valid
+  unsigned long long* phase_ns;  // optional per-phase time counters (nullptr = off)
 };
 
+// Phase counters (nanoseconds summed over warpgroups / roles):
+// 0 epilogue wait for the MMA, 1 row totals, 2 look-back, 3 drain,
+// 4 producer waits for free stages, 5 summer (including its waits for data),
+// 6 unused, 7 tiles processed.
+__device__ __forceinline__ void phase_add(const ScanParams& p, int k, uint64_t dt) {
+  if (p.phase_ns) atomicAdd(p.phase_ns + k, (unsigned long long)dt);
+}
+
 constexpr uint32_t kSentinel = 0xFFFFFFFFu;
-constexpr int kThreads = 320;  // 10 warps
+constexpr int kThreads = 352;  // 11 warps: producer, MMA, 2 epilogue warpgroups, summer
 constexpr int kMaxSmem = 232448;
 
 template <typename InT, int W>
@@ -66,8 +75,6 @@ struct ScanCfg {
   static constexpr int KB = RB / SW;                  // K blocks of SW bytes
   static constexpr int KSTEPS = SW / 32;              // 32-byte MMA K steps per block
   static constexpr int STAGE_BYTES = 128 * RB;
-  static constexpr int NSTAGE_RAW = 65536 / STAGE_BYTES;
-  static constexpr int NSTAGE = NSTAGE_RAW > 8 ? 8 : (NSTAGE_RAW < 2 ? 2 : NSTAGE_RAW);
   static constexpr int BPT = 256 / W;                 // blocks per tile
   static constexpr int TILE_ELEMS = 128 * 256;
   static constexpr int B_BYTES = W * RB;
@@ -76,23 +83,37 @@ struct ScanCfg {
   static constexpr int FILLW = W < 64 ? W : 64;       // columns staged per fill
   static constexpr int NFILL = W / FILLW;
   static constexpr int STG_BYTES = 128 * FILLW * 4;
+  // Shared memory: input stage ring | U | output staging | control.  The ring
+  // holds as many blocks as fit (at least one tile, at most four); output
+  // staging is double buffered unless that would leave under two tiles of
+  // input stages.
+  static constexpr int CTRL_BYTES = 3072;
+  static constexpr int B_ALLOC = ((B_BYTES + 1023) / 1024) * 1024;
+  static constexpr int FIXED = 1024 + CTRL_BYTES + B_ALLOC;
+  static constexpr int NST_DOUBLE = (kMaxSmem - FIXED - 4 * STG_BYTES) / STAGE_BYTES;
+  static constexpr int STG_BUFS = NST_DOUBLE >= 2 * BPT ? 2 : 1;
+  static constexpr int NST_FIT = (kMaxSmem - FIXED - 2 * STG_BUFS * STG_BYTES) / STAGE_BYTES;
+  static constexpr int NST_CAP = 4 * BPT < 32 ? 4 * BPT : 32;
+  static constexpr int NSTAGE = NST_FIT < NST_CAP ? NST_FIT : NST_CAP;
   static constexpr int OFF_B = NSTAGE * STAGE_BYTES;
-  static constexpr int OFF_STG = OFF_B + ((B_BYTES + 1023) / 1024) * 1024;
-  static constexpr int OFF_CTRL = OFF_STG + 4 * STG_BYTES;  // 2 warpgroups x 2 buffers
-  static constexpr int CTRL_BYTES = 2048;
+  static constexpr int OFF_STG = OFF_B + B_ALLOC;
+  static constexpr int OFF_CTRL = OFF_STG + 2 * STG_BUFS * STG_BYTES;
   static constexpr int SMEM_BYTES = OFF_CTRL + CTRL_BYTES + 1024;  // + alignment slack
+  static_assert(NSTAGE >= BPT, "stage ring must hold a whole tile");
   static_assert(W == 16 || W == 32 || W == 64 || W == 128, "S");
   static_assert(RB >= 32, "row must hold one 32-byte MMA K step");
   static_assert(SMEM_BYTES <= kMaxSmem, "shared memory budget");
 };
 
 struct ScanCtrl {
-  uint64_t full[8];
-  uint64_t empty[8];
+  uint64_t full[32];
+  uint64_t empty[32];
   uint64_t tile_full[2];
   uint64_t slot_empty[2][16];
   uint64_t drain;
-  uint32_t stage_cid[8];
+  uint64_t agg_full[8];             // summer -> epilogue: tile aggregate published
+  uint64_t agg_empty[8];            // epilogue -> summer: ring slot free
+  uint32_t stage_cid[32];
   uint32_t tile_cid[2];
   uint32_t tmem_base;
   uint32_t epoch;
@@ -102,7 +123,7 @@ struct ScanCtrl {
   uint8_t wt_flag[2][16][4];        // warp segment flags per block
   LbScratch lb[2];
 };
-static_assert(sizeof(ScanCtrl) <= 2048, "control block");
+static_assert(sizeof(ScanCtrl) <= 3072, "control block");
 
 // Value of 1 in the MMA operand encoding.
 template <typename T>
@@ -197,10 +218,12 @@ __device__ __forceinline__ void scan_epilogue(const ScanParams& p, const CUtenso
   const int r = q * 32 + lane;    // row within a block
   const int wg_thread = threadIdx.x - 64 - g * 128;
   const uint32_t bar_id = 1 + g;
-  uint8_t* stg_base = smem + C::OFF_STG + g * 2 * C::STG_BYTES;
+  uint8_t* stg_base = smem + C::OFF_STG + g * C::STG_BUFS * C::STG_BYTES;
   const V start = IS_INT ? (V)p.start_i : (V)p.start_f;
   uint32_t nfill = 0;
 
+  const bool prof = p.phase_ns != nullptr && wg_thread == 0;
+  uint64_t t_mark = prof ? globaltimer() : 0;
   for (uint32_t i = g;; i += 2) {
     const uint32_t u = i >> 1;
     // One lane per warp waits; the four warps then vote at a named barrier
@@ -213,6 +236,7 @@ __device__ __forceinline__ void scan_epilogue(const ScanParams& p, const CUtenso
     const int all_ok = ctl->wait_ok[g][0] & ctl->wait_ok[g][1] & ctl->wait_ok[g][2] & ctl->wait_ok[g][3];
     const uint32_t tid = *(volatile uint32_t*)&ctl->tile_cid[g];
     if (!all_ok || tid == kSentinel) break;
+    if (prof) { const uint64_t t = globaltimer(); phase_add(p, 0, t - t_mark); phase_add(p, 7, 1); t_mark = t; }
     tc_fence_after();
     const uint32_t tm = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(g * 256);
     const int64_t row_tile0 = (int64_t)tid * BPT * 128;
@@ -285,11 +309,18 @@ __device__ __forceinline__ void scan_epilogue(const ScanParams& p, const CUtenso
         rowex[j] = (MODE == kScanBlocks && fl[j]) ? V(0) : ex;
         if (bf) { run = bsum; runf = 1; } else { run += bsum; }
       }
+      if (prof) { const uint64_t t = globaltimer(); phase_add(p, 1, t - t_mark); t_mark = t; }
       if constexpr (MODE == kScanFull) {
-        const V pre = tile_lookback<V>((int64_t)tid, run, 0, start, p.descs, epoch, wc, &ctl->lb[g], wg_thread,
-                                       bar_id);
+        // The summer warp published this tile's aggregate as soon as its data
+        // landed; wait for that (ordering: the inclusive prefix must not be
+        // overwritten by a late aggregate), then look back.
+        const int m = i & 7;
+        if (wg_thread == 0) mbar_wait(&ctl->agg_full[m], (i >> 3) & 1u, wc, 6, i);
+        const V pre = wg_lookback<V>((int64_t)tid, run, start, p.descs, epoch, wc, &ctl->lb[g], wg_thread, bar_id);
+        if (wg_thread == 0) mbar_arrive(&ctl->agg_empty[m]);
 #pragma unroll
         for (int j = 0; j < BPT; ++j) rowex[j] = pre + rowex[j];
+        if (prof) { const uint64_t t = globaltimer(); phase_add(p, 2, t - t_mark); t_mark = t; }
       }
     }
 
@@ -304,8 +335,10 @@ __device__ __forceinline__ void scan_epilogue(const ScanParams& p, const CUtenso
       const uint32_t ci = IS_INT ? (uint32_t)(long long)rowex[j] : 0u;
 #pragma unroll
       for (int h = 0; h < C::NFILL; ++h) {
-        uint8_t* stg = stg_base + (nfill & 1u) * C::STG_BYTES;
-        if (wg_thread == 0) bulk_wait_read1();  // the store that last used this buffer has read it
+        uint8_t* stg = stg_base + (nfill % C::STG_BUFS) * C::STG_BYTES;
+        if (wg_thread == 0) {  // the store that last used this buffer has read it
+          if (C::STG_BUFS == 2) bulk_wait_read1(); else bulk_wait_read0();
+        }
         named_bar_sync(bar_id, 128);
         uint32_t v[C::FILLW];
 #pragma unroll
@@ -354,8 +387,100 @@ __device__ __forceinline__ void scan_epilogue(const ScanParams& p, const CUtenso
         ++nfill;
       }
     }
+    if (prof) { const uint64_t t = globaltimer(); phase_add(p, 3, t - t_mark); t_mark = t; }
   }
   if (wg_thread == 0) bulk_wait_all0();
+}
+
+// Summer warp: sums every tile straight from the TMA-filled SMEM stages (rows
+// past the input are skipped, the partial last row is read from global) and
+// publishes the tile aggregate at once, then hands (tile, aggregate) to the
+// look-back warp.  It never waits on another CTA, so a tile's aggregate is
+// visible about one TMA latency after the tile id was taken -- successors'
+// look-backs never queue behind this CTA's backlog.  For the row/block modes
+// it only releases the stages.
+template <typename InT, int W, int MODE>
+__device__ __forceinline__ void scan_summer(const ScanParams& p, uint8_t* smem, ScanCtrl* ctl, uint32_t epoch,
+                                                const WaitCtx& wc) {
+  using C = ScanCfg<InT, W>;
+  constexpr bool IS_INT = C::IS_INT;
+  constexpr int BPT = C::BPT;
+  using V = typename std::conditional<IS_INT, long long, double>::type;
+  const int lane = threadIdx.x & 31;
+  const V start = IS_INT ? (V)p.start_i : (V)p.start_f;
+  const bool prof = p.phase_ns != nullptr && lane == 0;
+  uint32_t k = 0;
+  uint32_t i = 0;
+  for (;; ++i) {
+    const uint64_t t0 = prof ? globaltimer() : 0;
+    bool stop = false;
+    uint32_t tid = 0;
+    float accf = 0.f;
+    int acci = 0;
+    for (int j = 0; j < BPT; ++j, ++k) {
+      const int s = k % C::NSTAGE;
+      // every lane observes the TMA barrier before reading the stage
+      const bool ok = __all_sync(0xffffffffu, mbar_wait(&ctl->full[s], (k / C::NSTAGE) & 1u, wc, 7, i));
+      if (!ok) { stop = true; break; }
+      const uint32_t cid = *(volatile uint32_t*)&ctl->stage_cid[s];
+      if (cid == kSentinel) { stop = true; break; }
+      tid = cid;
+      if constexpr (MODE == kScanFull) {
+        const int64_t row0 = ((int64_t)tid * BPT + j) * 128;
+        int64_t vr = p.full_rows - row0;
+        const int vrows = vr <= 0 ? 0 : (vr >= 128 ? 128 : (int)vr);
+        const int nv = vrows * (C::SW / 16);
+#pragma unroll
+        for (int kb = 0; kb < C::KB; ++kb) {
+          const uint4* src = (const uint4*)(smem + s * C::STAGE_BYTES + kb * (128 * C::SW));
+          for (int v = lane; v < nv; v += 32) {
+            const uint4 w = src[v];
+            if constexpr (IS_INT) {
+              acci = __dp4a((int)w.x, 0x01010101, acci);
+              acci = __dp4a((int)w.y, 0x01010101, acci);
+              acci = __dp4a((int)w.z, 0x01010101, acci);
+              acci = __dp4a((int)w.w, 0x01010101, acci);
+            } else {
+              const __half2* h = reinterpret_cast<const __half2*>(&w);
+#pragma unroll
+              for (int t = 0; t < 4; ++t) {
+                const float2 f = __half22float2(h[t]);
+                accf += f.x + f.y;
+              }
+            }
+          }
+        }
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&ctl->empty[s]);  // this consumer is done with the stage
+    }
+    if (stop) break;
+    if constexpr (MODE == kScanFull) {
+      const int64_t tile_row0 = (int64_t)tid * BPT * 128;
+      if (lane == 0 && p.tail > 0 && p.full_rows >= tile_row0 && p.full_rows < tile_row0 + BPT * 128) {
+        float af = 0.f;
+        int ai = 0;
+        uint32_t tmp[16];
+#pragma unroll
+        for (int c = 0; c < W / 16; ++c) tail_chunk<InT, W>(p, c * 16, tmp, af, ai);
+        accf += af;
+        acci += ai;
+      }
+      V agg;
+      if constexpr (IS_INT) agg = (V)warp_sum_any(acci);
+      else agg = warp_sum_any((double)accf);
+      int ok = 1;
+      if (lane == 0) {
+        publish_aggregate<V>((int64_t)tid, agg, 0, start, p.descs, epoch);
+        const int m = i & 7;
+        if (i >= 8) ok = mbar_wait(&ctl->agg_empty[m], ((i >> 3) & 1u) ^ 1u, wc, 8, i) ? 1 : 0;
+        if (ok) mbar_arrive(&ctl->agg_full[m]);
+      }
+      ok = __shfl_sync(0xffffffffu, ok, 0);
+      if (prof) phase_add(p, 5, globaltimer() - t0);
+      if (!ok) break;
+    }
+  }
 }
 
 template <typename InT, int W, int MODE>
@@ -379,7 +504,11 @@ __global__ void __launch_bounds__(kThreads, 1)
   if (threadIdx.x == 0) {
     for (int s = 0; s < C::NSTAGE; ++s) {
       mbar_init(&ctl->full[s], 1);
-      mbar_init(&ctl->empty[s], 1);
+      mbar_init(&ctl->empty[s], 2);  // MMA commit + aggregator arrive
+    }
+    for (int m = 0; m < 8; ++m) {
+      mbar_init(&ctl->agg_full[m], 1);
+      mbar_init(&ctl->agg_empty[m], 1);
     }
     for (int g = 0; g < 2; ++g) {
       mbar_init(&ctl->tile_full[g], 2);  // tcgen05.commit + releasing arrive after tile_cid
@@ -408,22 +537,31 @@ __global__ void __launch_bounds__(kThreads, 1)
 
   if (warp == 0) {
     // ================= TMA producer =================
+    // A tile id is taken only once every stage of that tile is free, and all
+    // of its blocks are then issued at once: the time from taking an id to
+    // its aggregate being published is one TMA round trip, never this CTA's
+    // backlog.
     if (lane == 0) {
-      uint32_t issued[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      uint32_t issued[32];
+#pragma unroll
+      for (int s = 0; s < 32; ++s) issued[s] = 0;
       uint32_t k = 0;  // block sequence number
-      uint32_t next = atomicAdd(&p.ws->tile_counter, 1u);
       bool stop = false;
       while (!stop) {
-        const uint32_t tid = next;
+        const uint64_t tw = p.phase_ns ? globaltimer() : 0;
+        for (int j = 0; j < BPT && !stop; ++j) {
+          const uint32_t kj = k + j;
+          const int s = kj % C::NSTAGE;
+          if (kj >= (uint32_t)C::NSTAGE && !mbar_wait(&ctl->empty[s], ((kj / C::NSTAGE) & 1u) ^ 1u, wc, 1, kj))
+            stop = true;
+        }
+        if (stop) break;
+        if (p.phase_ns) phase_add(p, 4, globaltimer() - tw);
+        const uint32_t tid = atomicAdd(&p.ws->tile_counter, 1u);
         const bool live = (int64_t)tid < p.num_tiles;
-        if (live) next = atomicAdd(&p.ws->tile_counter, 1u);
         const int nblk = live ? BPT : 1;
         for (int j = 0; j < nblk; ++j, ++k) {
           const int s = k % C::NSTAGE;
-          if (k >= (uint32_t)C::NSTAGE && !mbar_wait(&ctl->empty[s], ((k / C::NSTAGE) & 1u) ^ 1u, wc, 1, tid)) {
-            stop = true;
-            break;
-          }
           ctl->stage_cid[s] = live ? tid : kSentinel;
           issued[s]++;
           const int64_t row0 = ((int64_t)tid * BPT + j) * 128;
@@ -498,8 +636,10 @@ __global__ void __launch_bounds__(kThreads, 1)
       tc_commit(&ctl->drain);
       mbar_drain(&ctl->drain, 0, p.timeout_ns);
     }
-  } else {
+  } else if (warp < 10) {
     scan_epilogue<InT, W, MODE>(p, out_map, smem, ctl, tmem_base, epoch, wc);
+  } else {
+    scan_summer<InT, W, MODE>(p, smem, ctl, epoch, wc);
   }
 
   // ---- teardown ----

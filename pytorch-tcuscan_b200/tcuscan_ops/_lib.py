@@ -60,6 +60,8 @@ _sig("tcu_get_timeout_ns", _U64)
 _sig("tcu_workspace_bytes", _SZ, _I64, _I)
 _sig("tcu_workspace_init", _ST, _P, _SZ, _P)
 _sig("tcu_workspace_error", _ST, _P, ctypes.POINTER(ctypes.c_uint32), _I, _P)
+_sig("tcu_set_phase_profile", None, _I)
+_sig("tcu_workspace_phase_ns", _ST, _P, ctypes.POINTER(ctypes.c_uint64), _I, _P)
 _sig("tcu_scan", _ST, _P, _I, _I64, _I, _D, _P, _P, _SZ, _P)
 _sig("tcu_row_scan", _ST, _P, _I, _I64, _I, _P, _P, _SZ, _P)
 _sig("tcu_block_scan", _ST, _P, _I, _I64, _I, _P, _P, _SZ, _P)
@@ -149,3 +151,26 @@ def set_timeout_ns(ns):
 
 def get_timeout_ns():
     return int(lib.tcu_get_timeout_ns())
+
+
+PHASE_NAMES = ("epilogue_wait_mma", "row_totals", "lookback", "drain", "producer_wait_stage", "summer",
+               "unused", "tiles")
+
+
+def set_phase_profile(enable):
+    lib.tcu_set_phase_profile(int(bool(enable)))
+
+
+def phase_times(device=None, clear=True):
+    """Per-phase device time counters of the current stream's workspace (diagnostics)."""
+    dev = torch.device(device if device is not None else torch.cuda.current_device())
+    if dev.type == "cuda" and dev.index is None:
+        dev = torch.device("cuda", torch.cuda.current_device())
+    stream = torch.cuda.current_stream(dev)
+    ws = _workspaces.get((dev.index, stream.cuda_stream))
+    if ws is None or ws.buf is None:
+        return {}
+    out = (ctypes.c_uint64 * 8)()
+    check(lib.tcu_workspace_phase_ns(ctypes.c_void_p(ws.buf.data_ptr()), out, int(clear),
+                                     ctypes.c_void_p(stream.cuda_stream)), "tcu_workspace_phase_ns")
+    return {n: int(v) for n, v in zip(PHASE_NAMES, out)}
