@@ -99,6 +99,52 @@ TCU_API tcu_status_t tcu_row_scan(const void* x, tcu_dtype_t x_dtype, int64_t n_
 TCU_API tcu_status_t tcu_block_scan(const void* x, tcu_dtype_t x_dtype, int64_t n, int S, void* z, void* ws,
                             size_t ws_bytes, void* stream);
 
+/* ---- stream compaction ---------------------------------------------------
+ * Stable compaction of x[mask != 0] (elem_bytes = 1, 2, 4 or 8; int8 mask)
+ * in one pass with a decoupled look-back; selected elements beyond
+ * `capacity` are dropped.  idx_mode 0: values only; 1: also gather idx_in
+ * (idx_bytes = 4 or 8); 2: also write the selected positions (int32 when
+ * idx_bytes = 4, int64 when 8).  count_dev (optional, 8-byte aligned device
+ * int64) receives the number selected.
+ * Replaces run_compress (src/torch/torch_compress.h:41-98), run_compress_pos
+ * (:109-161, capacity = output_len), run_compress_ind (:172-239) and
+ * run_compress_ind_no_arange (:249-309).                                   */
+TCU_API tcu_status_t tcu_compress(const void* x, int elem_bytes, const int8_t* mask, int64_t n, const void* idx_in,
+                                  int idx_bytes, int idx_mode, void* out, void* idx_out, int64_t capacity,
+                                  void* count_dev, void* ws, size_t ws_bytes, void* stream);
+/* Number of mask != 0 into a device uint64 (the reference sizes compress
+ * outputs with run_reduce_tiles + .sum(), src/torch/torch_compress.h:62-64). */
+TCU_API tcu_status_t tcu_mask_count(const int8_t* mask, int64_t n, void* count_dev, void* stream);
+
+/* ---- CSR gather ------------------------------------------------------------
+ * z[i] = values[i] * x[cols[i]] in the values dtype (fp16, int16, fp32).
+ * Out-of-range columns read 0 and record TCU_ERR_ARG in ws (optional).
+ * Replaces run_csr_gather (src/torch/torch_gather.h:92-172).               */
+TCU_API tcu_status_t tcu_csr_gather(const void* values, tcu_dtype_t dtype, const int32_t* cols, int64_t nnz,
+                                    const void* x, int64_t x_len, void* z, void* ws, void* stream);
+
+/* ---- scan phases as standalone operators ----------------------------------
+ * reduce_tiles: z[b] = sum of block b, block = tile_len * ceil(ceil(n /
+ * tile_len) / num_blocks) elements; int8 -> int32, fp16 -> fp32.  Needs
+ * 128 + 8 * num_blocks * 64 bytes of workspace.
+ * Replaces run_reduce_tiles (src/torch/torch_reduce.h:42-75).             */
+TCU_API tcu_status_t tcu_reduce_tiles(const void* x, tcu_dtype_t dtype, int64_t n, int64_t tile_len, int num_blocks,
+                                      void* z, void* ws, size_t ws_bytes, void* stream);
+/* complete_rows: block b (n / num_blocks elements) starts from sum(sums[:b]);
+ * each `width`-long row gets the running carry added, and the carry becomes
+ * the updated row's last element.  fp32 or int32.  Workspace: 128 + 8 *
+ * num_blocks * ceil(block / width) bytes.
+ * Replaces run_complete_rows (src/torch/torch_reduce.h:143-182).          */
+TCU_API tcu_status_t tcu_complete_rows(const void* x, tcu_dtype_t dtype, int64_t n, const void* sums, int num_blocks,
+                                       int64_t width, void* z, void* ws, size_t ws_bytes, void* stream);
+/* complete_blocks: z[block b] = x[block b] + sum(sums[:b]); fp32 or int32.
+ * Replaces run_complete_blocks (src/torch/torch_reduce.h:197-231).        */
+TCU_API tcu_status_t tcu_complete_blocks(const void* x, tcu_dtype_t dtype, int64_t n, const void* sums,
+                                         int num_blocks, void* z, void* stream);
+/* z = tril(ones(s, s)) in int8 / fp16 / bf16 / fp32 / int32.
+ * Replaces run_gen_lower (src/torch/torch_gen_lower.h:31-59).            */
+TCU_API tcu_status_t tcu_gen_lower(int64_t s, tcu_dtype_t dtype, void* z, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

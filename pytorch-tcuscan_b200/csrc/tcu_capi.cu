@@ -211,9 +211,9 @@ void tcu_set_timeout_ns(uint64_t ns) { g_timeout_ns = ns ? ns : 4000000000ull; }
 uint64_t tcu_get_timeout_ns(void) { return g_timeout_ns; }
 
 size_t tcu_workspace_bytes(int64_t n, int S) {
-  (void)S;  // a tile is 32768 elements for every S
+  (void)S;  // the smallest look-back tile of any kernel is 4096 elements
   if (n < 0) n = 0;
-  const int64_t tiles = (n + 32767) / 32768 + 2;
+  const int64_t tiles = (n + 4095) / 4096 + 2;
   return 128 + (size_t)tiles * sizeof(TileDesc);
 }
 

@@ -155,8 +155,241 @@ def run_block_scan(x, upper, lower_strict):
 
 
 def run_gen_lower(matrix_size, device, dtype):
-    """torch.tril(ones(s, s)) (reference: src/torch/torch_gen_lower.h:31-59)."""
-    return torch.tril(torch.ones((int(matrix_size), int(matrix_size)), dtype=dtype, device=device))
+    """tril(ones(s, s)) on the device (reference: src/torch/torch_gen_lower.h:31-59)."""
+    s_ = int(matrix_size)
+    dev = torch.device(device)
+    z = torch.empty((s_, s_), dtype=dtype, device=dev)
+    if dtype not in _lib.DTYPE_CODE:
+        raise TypeError(f"run_gen_lower: unsupported dtype {dtype}")
+    check(_lib.lib.tcu_gen_lower(s_, _lib.DTYPE_CODE[dtype], z.data_ptr(), stream_ptr(dev)), "run_gen_lower")
+    return z
+
+
+# ---------------------------------------------------------------------------
+# stream compaction (src/torch/torch_compress.h)
+
+def _mask_input(mask, n, x_device):
+    mask = _cuda_input(mask, "mask")
+    if mask.device != x_device:
+        raise ValueError("mask must be on the device of x")
+    if mask.dtype in (torch.bool, torch.uint8):
+        mask = mask.view(torch.int8)
+    if mask.dtype != torch.int8:
+        raise TypeError(f"mask must be int8 (or bool/uint8), got {mask.dtype}")
+    if mask.numel() != n:
+        raise ValueError(f"mask has {mask.numel()} elements, x has {n}")
+    return mask
+
+
+def _count(mask):
+    n = mask.numel()
+    cnt = torch.empty(1, dtype=torch.int64, device=mask.device)
+    check(_lib.lib.tcu_mask_count(mask.data_ptr(), n, cnt.data_ptr(), stream_ptr(mask.device)), "mask count")
+    return cnt
+
+
+def _compress(x, mask, out_len, idx_in=None, idx_mode=0, idx_dtype=torch.int32, where="run_compress"):
+    n = x.numel()
+    z = torch.empty(out_len, dtype=x.dtype, device=x.device)
+    idx_out = None
+    ib = 0
+    if idx_mode == 1:
+        idx_out = torch.empty(out_len, dtype=idx_in.dtype, device=x.device)
+        ib = idx_in.element_size()
+    elif idx_mode == 2:
+        idx_out = torch.empty(out_len, dtype=idx_dtype, device=x.device)
+        ib = idx_out.element_size()
+    if n == 0:
+        return z, idx_out
+    ws, wsb = workspace(x.device, _lib.lib.tcu_workspace_bytes(n, 64))
+    st = _lib.lib.tcu_compress(
+        x.data_ptr(), x.element_size(), mask.data_ptr(), n,
+        idx_in.data_ptr() if idx_in is not None else None, ib, idx_mode,
+        z.data_ptr() if out_len > 0 else x.data_ptr(),
+        (idx_out.data_ptr() if out_len > 0 else x.data_ptr()) if idx_out is not None else None,
+        out_len, None, ws, wsb, stream_ptr(x.device))
+    check(st, where)
+    _after(x)
+    return z, idx_out
+
+
+def _check_S_opt(S):
+    if S is not None and int(S) != 0:
+        _pick_S(S, torch.float16)
+
+
+def run_compress(x, mask, S):
+    """Stable x[mask != 0] (reference: src/torch/torch_compress.h:41-98).
+
+    The reference selects mask == 1 and sizes the output with sum(mask); both
+    agree for 0/1 masks.  One count pass (read back to size the output, as
+    the reference does) and one single-pass compaction kernel."""
+    _check_S_opt(S)
+    x = _cuda_input(x)
+    mask = _mask_input(mask, x.numel(), x.device)
+    k = int(_count(mask).item())
+    return _compress(x, mask, k)[0]
+
+
+def run_compress_pos(x, mask, output_len, S):
+    """Compaction into an output of the given length (reference:
+    src/torch/torch_compress.h:109-161); no host round trip."""
+    _check_S_opt(S)
+    x = _cuda_input(x)
+    mask = _mask_input(mask, x.numel(), x.device)
+    return _compress(x, mask, int(output_len), where="run_compress_pos")[0]
+
+
+def run_compress_ind(x, indices_in, mask, S):
+    """(x[mask], indices_in[mask]) (reference: src/torch/torch_compress.h:172-239)."""
+    _check_S_opt(S)
+    x = _cuda_input(x)
+    indices_in = _cuda_input(indices_in, "indices_in")
+    if indices_in.numel() != x.numel():
+        raise ValueError("indices_in must have the length of x")
+    if indices_in.element_size() not in (4, 8):
+        raise TypeError("indices_in must be a 32- or 64-bit integer tensor")
+    mask = _mask_input(mask, x.numel(), x.device)
+    k = int(_count(mask).item())
+    z, idx = _compress(x, mask, k, idx_in=indices_in, idx_mode=1, where="run_compress_ind")
+    return z, idx
+
+
+def run_compress_ind_no_arange(x, mask, S):
+    """(x[mask], positions of the selected elements as int32) (reference:
+    src/torch/torch_compress.h:249-309)."""
+    _check_S_opt(S)
+    x = _cuda_input(x)
+    mask = _mask_input(mask, x.numel(), x.device)
+    k = int(_count(mask).item())
+    return _compress(x, mask, k, idx_mode=2, where="run_compress_ind_no_arange")
+
+
+def run_filter_greater_eq(x, pivot, S):
+    """x[x >= pivot] (reference: src/torch/torch_compress.h:319-323)."""
+    x = _cuda_input(x)
+    return run_compress(x, (x >= pivot).to(torch.int8), S)
+
+
+def run_filter_less_eq(x, pivot, S):
+    """x[x <= pivot] (reference: src/torch/torch_compress.h:333-337)."""
+    x = _cuda_input(x)
+    return run_compress(x, (x <= pivot).to(torch.int8), S)
+
+
+def run_where(x, pivot, S):
+    """int32 positions where x >= pivot (reference: src/torch/torch_compress.h:347-398)."""
+    x = _cuda_input(x)
+    return run_compress_ind_no_arange(x, (x >= pivot).to(torch.int8), S)[1]
+
+
+# ---------------------------------------------------------------------------
+# gather (src/torch/torch_gather.h)
+
+def run_csr_gather(values, cols, x):
+    """z[i] = values[i] * x[cols[i]] in the values dtype (reference:
+    src/torch/torch_gather.h:92-172, same argument checks).  x is read
+    through L2, so unlike the reference it is not limited to what fits on
+    chip."""
+    if values.dim() != 1:
+        raise ValueError(f"run_csr_gather: values must be 1D, got {values.dim()}D")
+    if cols.dim() != 1:
+        raise ValueError(f"run_csr_gather: cols must be 1D, got {cols.dim()}D")
+    if x.dim() != 1:
+        raise ValueError(f"run_csr_gather: x must be 1D, got {x.dim()}D")
+    if cols.numel() != values.numel():
+        raise ValueError(f"run_csr_gather: cols length ({cols.numel()}) must match values length ({values.numel()})")
+    if values.dtype not in (torch.float16, torch.int16, torch.float32):
+        raise TypeError(f"run_csr_gather: values dtype must be fp16, int16, or fp32, got {values.dtype}")
+    if x.dtype != values.dtype:
+        raise TypeError(f"run_csr_gather: x dtype ({x.dtype}) must match values dtype ({values.dtype})")
+    if cols.dtype != torch.int32:
+        raise TypeError(f"run_csr_gather: cols dtype must be int32, got {cols.dtype}")
+    if not (values.is_contiguous() and cols.is_contiguous() and x.is_contiguous()):
+        raise ValueError("run_csr_gather: values, cols and x must be contiguous")
+    if values.device != cols.device or values.device != x.device:
+        raise ValueError("run_csr_gather: values, cols and x must be on the same device")
+    values, cols, x = _cuda_input(values, "values"), _cuda_input(cols, "cols"), _cuda_input(x)
+    z = torch.empty_like(values)
+    nnz = values.numel()
+    if nnz == 0:
+        return z
+    ws, _ = workspace(x.device, 1 << 20)
+    st = _lib.lib.tcu_csr_gather(values.data_ptr(), _lib.DTYPE_CODE[values.dtype], cols.data_ptr(), nnz,
+                                 x.data_ptr(), x.numel(), z.data_ptr(), ws, stream_ptr(x.device))
+    check(st, "run_csr_gather")
+    _after(x)
+    return z
+
+
+# ---------------------------------------------------------------------------
+# scan phases as standalone operators (src/torch/torch_reduce.h)
+
+def run_reduce_tiles(x, tile_len, num_blocks):
+    """Per-block sums (reference: src/torch/torch_reduce.h:42-75):
+    block = tile_len * ceil(ceil(n / tile_len) / num_blocks) elements;
+    int8 -> int32, float16 -> float32."""
+    x = _cuda_input(x)
+    if x.dtype not in (torch.int8, torch.float16):
+        raise TypeError(f"run_reduce_tiles: x must be int8 or float16, got {x.dtype}")
+    tile_len, num_blocks = int(tile_len), int(num_blocks)
+    if tile_len <= 0 or num_blocks <= 0:
+        raise ValueError("run_reduce_tiles: tile_len and num_blocks must be positive")
+    z = torch.empty(num_blocks, dtype=_scan_out_dtype(x.dtype), device=x.device)
+    ws, wsb = workspace(x.device, 128 + 8 * num_blocks * 64)
+    st = _lib.lib.tcu_reduce_tiles(x.data_ptr(), _lib.DTYPE_CODE[x.dtype], x.numel(), tile_len, num_blocks,
+                                   z.data_ptr(), ws, wsb, stream_ptr(x.device))
+    check(st, "run_reduce_tiles")
+    _after(x)
+    return z
+
+
+def run_complete_rows(x, sums, tile_width, tile_height):
+    """MCSCAN down-sweep over rows (reference: src/torch/torch_reduce.h:143-182,
+    semantics of tests/test_complete_rows.py ref_complete_rows).  x float32 ->
+    float32, int32 -> int32 (the reference routes int64 keys to its int32
+    kernel; here int64 is rejected)."""
+    x = _cuda_input(x)
+    sums = _cuda_input(sums, "sums")
+    if x.dtype not in (torch.float32, torch.int32):
+        raise TypeError(f"run_complete_rows: x must be float32 or int32, got {x.dtype}")
+    sums = sums.to(x.dtype)
+    nb = sums.numel()
+    n = x.numel()
+    if nb == 0 or n % nb != 0:
+        raise ValueError("run_complete_rows: len(x) must be a multiple of len(sums)")
+    width = int(tile_width)
+    rows = (n // nb + width - 1) // width
+    z = torch.empty(n, dtype=x.dtype, device=x.device)
+    if n == 0:
+        return z
+    ws, wsb = workspace(x.device, 128 + 8 * nb * rows)
+    st = _lib.lib.tcu_complete_rows(x.data_ptr(), _lib.DTYPE_CODE[x.dtype], n, sums.data_ptr(), nb, width,
+                                    z.data_ptr(), ws, wsb, stream_ptr(x.device))
+    check(st, "run_complete_rows")
+    _after(x)
+    return z
+
+
+def run_complete_blocks(x, sums, tile_length):
+    """z[block b] = x[block b] + sum(sums[:b]) (reference:
+    src/torch/torch_reduce.h:197-231).  float32 or int32."""
+    x = _cuda_input(x)
+    sums = _cuda_input(sums, "sums")
+    if x.dtype not in (torch.float32, torch.int32):
+        raise TypeError(f"run_complete_blocks: x must be float32 or int32, got {x.dtype}")
+    sums = sums.to(x.dtype)
+    nb, n = sums.numel(), x.numel()
+    if nb == 0 or n % nb != 0:
+        raise ValueError("run_complete_blocks: len(x) must be a multiple of len(sums)")
+    z = torch.empty_like(x)
+    if n == 0:
+        return z
+    st = _lib.lib.tcu_complete_blocks(x.data_ptr(), _lib.DTYPE_CODE[x.dtype], n, sums.data_ptr(), nb, z.data_ptr(),
+                                      stream_ptr(x.device))
+    check(st, "run_complete_blocks")
+    _after(x)
+    return z
 
 
 def run_scan_cpu(x):

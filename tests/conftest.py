@@ -22,12 +22,14 @@ def golden():
 
 
 def _ensure_lib():
-    """Build libtcuscan.so in-tree when it is missing (nvcc cross-compiles on CPU)."""
+    """Build libtcuscan.so in-tree when it is missing or older than its sources
+    (nvcc cross-compiles on CPU; incremental).  On a machine without nvcc the
+    prebuilt library is used as is."""
     lib = os.path.join(PKG, "lib", "libtcuscan.so")
-    if not os.path.exists(lib):
-        sys.path.insert(0, PKG)
-        import build as _b
+    sys.path.insert(0, PKG)
+    import build as _b
 
+    if not os.path.exists(lib) or os.path.exists(_b.NVCC):
         _b.build()
     return lib
 
