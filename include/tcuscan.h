@@ -99,6 +99,28 @@ TCU_API tcu_status_t tcu_row_scan(const void* x, tcu_dtype_t x_dtype, int64_t n_
 TCU_API tcu_status_t tcu_block_scan(const void* x, tcu_dtype_t x_dtype, int64_t n, int S, void* z, void* ws,
                             size_t ws_bytes, void* stream);
 
+/* ---- segmented scans (tensor cores) ---------------------------------------
+ * Segmented inclusive scan of x (int8 -> int32 exact, fp16 -> fp32).
+ * flags_are_ends = 0: flags[i] != 0 starts a segment at i (run_seg_scan,
+ * src/torch/torch_seg_ops.h:165-193); 1: flags[i] != 0 ends a segment at i,
+ * the building block of run_seg_sum (:85-107).  S in {16,32,64,128} (tiles of
+ * 32 or 64 columns are used; results do not depend on S).                  */
+TCU_API tcu_status_t tcu_seg_scan(const void* x, tcu_dtype_t x_dtype, int64_t n, int S, const int8_t* flags,
+                                  int flags_are_ends, void* z, void* ws, size_t ws_bytes, void* stream);
+/* Segments given by a non-decreasing start array bounds[0..nbounds) (int32 or
+ * int64; a CSR indptr).  out_sums = 1: out[k] = sum x[bounds[k]:bounds[k+1]]
+ * for k < nbounds-1 (empty segments give 0) -- run_seg_sum_multi_core
+ * (src/torch/torch_seg_ops.h:333-426), _single_core (:211-266), _multi_cube
+ * (:443-522), _single_cube (:278-322, starts + n).  out_sums = 0: out is the
+ * segmented scan of all n elements (uneven batched rows).                  */
+TCU_API tcu_status_t tcu_seg_bounds(const void* x, tcu_dtype_t x_dtype, int64_t n, int S, const void* bounds,
+                                    tcu_dtype_t bounds_dtype, int64_t nbounds, int out_sums, void* out, void* ws,
+                                    size_t ws_bytes, void* stream);
+/* Row-wise scan of a row-major [batch, len] matrix (int8 / fp16).
+ * Replaces run_scan_batch (src/torch/torch_scan.h:119-175).               */
+TCU_API tcu_status_t tcu_scan_batch(const void* x, tcu_dtype_t x_dtype, int64_t batch, int64_t len, int S, void* z,
+                                    void* ws, size_t ws_bytes, void* stream);
+
 /* ---- stream compaction ---------------------------------------------------
  * Stable compaction of x[mask != 0] (elem_bytes = 1, 2, 4 or 8; int8 mask)
  * in one pass with a decoupled look-back; selected elements beyond

@@ -90,10 +90,22 @@ unsigned long long* ws_phase_counters(void* ws) {
 
 // ---------------------------------------------------------------------------
 // Tensor-core scan launcher.
+// Segment description of the segmented modes (unused fields stay zero).
+struct SegArgs {
+  const int8_t* flags = nullptr;
+  const void* bounds = nullptr;
+  int64_t nbounds = 0;
+  int bounds64 = 0;
+  int out_sums = 0;
+  int64_t period = 0;
+  void* seg_out = nullptr;
+};
+
 template <typename InT, int W, int MODE>
 static tcu_status_t launch_scan_tc(const void* x, int64_t n, void* z, double start_f, long long start_i,
-                                   int seg_rows, void* ws, size_t ws_bytes, cudaStream_t st) {
-  using C = ScanCfg<InT, W>;
+                                   int seg_rows, void* ws, size_t ws_bytes, cudaStream_t st,
+                                   const SegArgs& sa = SegArgs()) {
+  using C = ScanCfg<InT, W, is_seg(MODE)>;
   ScanParams p{};
   p.x = x;
   p.z = z;
@@ -116,6 +128,13 @@ static tcu_status_t launch_scan_tc(const void* x, int64_t n, void* z, double sta
   p.ws = static_cast<WsHeader*>(ws);
   p.descs = ws_descs(ws);
   p.phase_ns = g_phase_profile ? ws_phase_counters(ws) : nullptr;
+  p.flags = sa.flags;
+  p.bounds = sa.bounds;
+  p.nbounds = sa.nbounds;
+  p.bounds64 = sa.bounds64;
+  p.out_sums = sa.out_sums;
+  p.period = sa.period;
+  p.seg_out = sa.seg_out;
 
   CUtensorMap in_map, out_map;
   std::memset(&in_map, 0, sizeof(in_map));
@@ -125,8 +144,10 @@ static tcu_status_t launch_scan_tc(const void* x, int64_t n, void* z, double sta
     const CUtensorMapDataType idt = C::IS_INT ? CU_TENSOR_MAP_DATA_TYPE_UINT8 : CU_TENSOR_MAP_DATA_TYPE_UINT16;
     tcu_status_t s = make_map_2d(&in_map, x, idt, C::ELEM, W, (uint64_t)p.full_rows, C::SW / C::ELEM, 128);
     if (s != TCU_OK) return s;
-    s = make_map_2d(&out_map, z, CU_TENSOR_MAP_DATA_TYPE_UINT32, 4, W, (uint64_t)p.full_rows, C::OBW, 128);
-    if (s != TCU_OK) return s;
+    if (z != nullptr) {
+      s = make_map_2d(&out_map, z, CU_TENSOR_MAP_DATA_TYPE_UINT32, 4, W, (uint64_t)p.full_rows, C::OBW, 128);
+      if (s != TCU_OK) return s;
+    }
   }
   const int smem = C::SMEM_BYTES < 120 * 1024 ? 120 * 1024 : C::SMEM_BYTES;
   auto kern = scan_tc_kernel<InT, W, MODE>;
@@ -164,6 +185,21 @@ static tcu_status_t dispatch_scan(const void* x, tcu_dtype_t dt, int64_t n, int 
       case 128: return launch_scan_tc<__half, 128, MODE>(x, n, z, start, 0, seg_rows, ws, ws_bytes, st);
       default: return TCU_ERR_ARG;
     }
+  }
+  return TCU_ERR_DTYPE;
+}
+
+template <int MODE>
+static tcu_status_t dispatch_seg(const void* x, tcu_dtype_t dt, int64_t n, int S, void* z, const SegArgs& sa, void* ws,
+                                 size_t ws_bytes, cudaStream_t st) {
+  const int W = S <= 32 ? 32 : 64;  // segmented results do not depend on the tile width
+  if (dt == TCU_INT8) {
+    if (W == 32) return launch_scan_tc<int8_t, 32, MODE>(x, n, z, 0.0, 0, 0, ws, ws_bytes, st, sa);
+    return launch_scan_tc<int8_t, 64, MODE>(x, n, z, 0.0, 0, 0, ws, ws_bytes, st, sa);
+  }
+  if (dt == TCU_FLOAT16) {
+    if (W == 32) return launch_scan_tc<__half, 32, MODE>(x, n, z, 0.0, 0, 0, ws, ws_bytes, st, sa);
+    return launch_scan_tc<__half, 64, MODE>(x, n, z, 0.0, 0, 0, ws, ws_bytes, st, sa);
   }
   return TCU_ERR_DTYPE;
 }
@@ -258,6 +294,53 @@ tcu_status_t tcu_row_scan(const void* x, tcu_dtype_t x_dtype, int64_t n_rows, in
   if (!x || !z) return TCU_ERR_ARG;
   if (!aligned16(x) || !aligned16(z)) return TCU_ERR_ALIGN;
   return dispatch_scan<kScanRows>(x, x_dtype, n_rows * S, S, z, 0.0, 0, ws, ws_bytes, (cudaStream_t)stream);
+}
+
+tcu_status_t tcu_seg_scan(const void* x, tcu_dtype_t x_dtype, int64_t n, int S, const int8_t* flags, int flags_are_ends,
+                          void* z, void* ws, size_t ws_bytes, void* stream) {
+  if (n < 0) return TCU_ERR_ARG;
+  if (n == 0) return TCU_OK;
+  if (!x || !z || !flags) return TCU_ERR_ARG;
+  if (!aligned16(x) || !aligned16(z) || !aligned16(flags)) return TCU_ERR_ALIGN;
+  SegArgs sa;
+  sa.flags = flags;
+  if (flags_are_ends)
+    return dispatch_seg<kSegEnds>(x, x_dtype, n, S, z, sa, ws, ws_bytes, (cudaStream_t)stream);
+  return dispatch_seg<kSegFlags>(x, x_dtype, n, S, z, sa, ws, ws_bytes, (cudaStream_t)stream);
+}
+
+tcu_status_t tcu_seg_bounds(const void* x, tcu_dtype_t x_dtype, int64_t n, int S, const void* bounds,
+                            tcu_dtype_t bounds_dtype, int64_t nbounds, int out_sums, void* out, void* ws,
+                            size_t ws_bytes, void* stream) {
+  if (n < 0 || nbounds < 0) return TCU_ERR_ARG;
+  if (bounds_dtype != TCU_INT32 && bounds_dtype != TCU_INT64) return TCU_ERR_DTYPE;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (out_sums && nbounds >= 2 && n == 0) {
+    cudaError_t e = cudaMemsetAsync(out, 0, (size_t)(nbounds - 1) * 4, st);
+    return e == cudaSuccess ? TCU_OK : cuda_fail(e, "cudaMemsetAsync(empty seg sums)");
+  }
+  if (n == 0 || (out_sums && nbounds < 2)) return TCU_OK;
+  if (!x || !out || !bounds || nbounds < 1) return TCU_ERR_ARG;
+  if (!aligned16(x) || !aligned16(out)) return TCU_ERR_ALIGN;
+  if ((reinterpret_cast<uintptr_t>(bounds) & (bounds_dtype == TCU_INT64 ? 7u : 3u)) != 0) return TCU_ERR_ALIGN;
+  SegArgs sa;
+  sa.bounds = bounds;
+  sa.nbounds = nbounds;
+  sa.bounds64 = bounds_dtype == TCU_INT64;
+  sa.out_sums = out_sums ? 1 : 0;
+  sa.seg_out = out_sums ? out : nullptr;
+  return dispatch_seg<kSegBounds>(x, x_dtype, n, S, out_sums ? nullptr : out, sa, ws, ws_bytes, st);
+}
+
+tcu_status_t tcu_scan_batch(const void* x, tcu_dtype_t x_dtype, int64_t batch, int64_t len, int S, void* z, void* ws,
+                            size_t ws_bytes, void* stream) {
+  if (batch < 0 || len < 0) return TCU_ERR_ARG;
+  if (batch == 0 || len == 0) return TCU_OK;
+  if (!x || !z) return TCU_ERR_ARG;
+  if (!aligned16(x) || !aligned16(z)) return TCU_ERR_ALIGN;
+  SegArgs sa;
+  sa.period = len;
+  return dispatch_seg<kSegPeriodic>(x, x_dtype, batch * len, S, z, sa, ws, ws_bytes, (cudaStream_t)stream);
 }
 
 tcu_status_t tcu_block_scan(const void* x, tcu_dtype_t x_dtype, int64_t n, int S, void* z, void* ws,

@@ -66,12 +66,6 @@ __device__ __forceinline__ typename ElemT<EB>::T vec_elem(const uint4* v, int j)
   }
 }
 
-// 4 mask bytes -> 4 selection bits (byte != 0).
-__device__ __forceinline__ uint32_t sel4(uint32_t w) {
-  const uint32_t u = __vsetne4(w, 0u);  // 0x01 per nonzero byte
-  return (u & 1u) | ((u >> 7) & 2u) | ((u >> 14) & 4u) | ((u >> 21) & 8u);
-}
-
 // IDX: 0 none, 1 gather idx_in (IB bytes), 2 positions (int32 when IB == 4,
 // int64 when IB == 8).
 template <int EB, int IDX, int IB, int E>

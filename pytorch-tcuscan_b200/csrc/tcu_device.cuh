@@ -12,6 +12,8 @@
 #include <cuda_fp16.h>
 #include <stdint.h>
 
+#include <climits>
+
 #include "tcuscan.h"
 
 namespace tcu {
@@ -245,6 +247,12 @@ __device__ __forceinline__ V warp_sum_any(V v) {
   return v;
 }
 __device__ __forceinline__ void bulk_wait_read1() { asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory"); }
+
+// 4 mask bytes -> 4 selection bits (byte != 0).
+__device__ __forceinline__ uint32_t sel4(uint32_t w) {
+  const uint32_t u = __vsetne4(w, 0u);  // 0x01 per nonzero byte
+  return (u & 1u) | ((u >> 7) & 2u) | ((u >> 14) & 4u) | ((u >> 21) & 8u);
+}
 
 // 32 lanes x 32 bit, one column per thread.
 __device__ __forceinline__ uint32_t tmem_ld1(uint32_t taddr) {

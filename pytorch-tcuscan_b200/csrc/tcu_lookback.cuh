@@ -137,7 +137,8 @@ struct LbScratch {
 // warp; this publishes the inclusive prefix agg_inc + exclusive prefix.
 template <typename V>
 __device__ __forceinline__ V wg_lookback(int64_t tid, V agg_inc, V start, TileDesc* descs, uint32_t epoch,
-                                         const WaitCtx& wc, LbScratch* sc, int wg_thread, uint32_t bar_id) {
+                                         const WaitCtx& wc, LbScratch* sc, int wg_thread, uint32_t bar_id,
+                                         int agg_seg = 0) {
   if (tid == 0) return start;
   const int lane = wg_thread & 31, q = wg_thread >> 5;
   const uint32_t tag = (epoch & 0x1FFFFFFFu) << 3;
@@ -200,7 +201,8 @@ __device__ __forceinline__ V wg_lookback(int64_t tid, V agg_inc, V start, TileDe
     if (dmin != 0xFFFFFFFFu) break;
     base -= 128 * K;
   }
-  if (wg_thread == 0) desc_store(descs + tid, v_bits<V>(acc + agg_inc), tag | LB_INC);
+  if (wg_thread == 0)
+    desc_store(descs + tid, v_bits<V>(agg_seg ? agg_inc : acc + agg_inc), tag | (agg_seg ? LB_SEGSTART : 0u) | LB_INC);
   return acc;
 }
 

@@ -32,10 +32,15 @@
 namespace tcu {
 
 enum ScanMode : int {
-  kScanFull = 0,    // full inclusive scan with look-back carries (MCSCAN)
-  kScanRows = 1,    // per-row (length S) scans only (row_scan)
-  kScanBlocks = 2,  // scans restarting every seg_rows rows (block_scan)
+  kScanFull = 0,     // full inclusive scan with look-back carries (MCSCAN)
+  kScanRows = 1,     // per-row (length S) scans only (row_scan)
+  kScanBlocks = 2,   // scans restarting every seg_rows rows (block_scan)
+  kSegFlags = 3,     // segmented scan, int8 flags mark segment starts (seg_scan)
+  kSegEnds = 4,      // segmented scan, int8 flags mark segment ends (seg_sum)
+  kSegBounds = 5,    // segments from a sorted start array (indptr / offsets)
+  kSegPeriodic = 6,  // segments of a fixed length (scan_batch)
 };
+constexpr bool is_seg(int mode) { return mode >= kSegFlags; }
 
 struct ScanParams {
   const void* x;      // input base (tail row loads)
@@ -52,6 +57,14 @@ struct ScanParams {
   uint64_t timeout_ns;
   int has_map;        // full_rows > 0: TMA maps are valid
   unsigned long long* phase_ns;  // optional per-phase time counters (nullptr = off)
+  // segmented modes
+  const int8_t* flags;   // kSegFlags / kSegEnds
+  const void* bounds;    // kSegBounds: non-decreasing segment starts
+  int64_t nbounds;
+  int bounds64;          // bounds are int64 (else int32)
+  int out_sums;          // kSegBounds: write one sum per segment instead of the scan
+  int64_t period;        // kSegPeriodic
+  void* seg_out;         // kSegBounds sums: nbounds - 1 entries (fp32 / int32)
 };
 
 // Phase counters (nanoseconds summed over warpgroups / roles):
@@ -66,7 +79,7 @@ constexpr uint32_t kSentinel = 0xFFFFFFFFu;
 constexpr int kThreads = 352;  // 11 warps: producer, MMA, 2 epilogue warpgroups, summer
 constexpr int kMaxSmem = 232448;
 
-template <typename InT, int W>
+template <typename InT, int W, bool SEG = false>
 struct ScanCfg {
   static constexpr int ELEM = (int)sizeof(InT);
   static constexpr bool IS_INT = (ELEM == 1);
@@ -89,7 +102,9 @@ struct ScanCfg {
   // input stages.
   static constexpr int CTRL_BYTES = 3072;
   static constexpr int B_ALLOC = ((B_BYTES + 1023) / 1024) * 1024;
-  static constexpr int FIXED = 1024 + CTRL_BYTES + B_ALLOC;
+  // segmented modes keep one 64-bit start mask per row of a tile per warpgroup
+  static constexpr int MASK_BYTES = SEG ? 2 * BPT * 128 * 8 : 0;
+  static constexpr int FIXED = 1024 + CTRL_BYTES + B_ALLOC + MASK_BYTES;
   static constexpr int NST_DOUBLE = (kMaxSmem - FIXED - 4 * STG_BYTES) / STAGE_BYTES;
   static constexpr int STG_BUFS = NST_DOUBLE >= 2 * BPT ? 2 : 1;
   static constexpr int NST_FIT = (kMaxSmem - FIXED - 2 * STG_BUFS * STG_BYTES) / STAGE_BYTES;
@@ -97,9 +112,11 @@ struct ScanCfg {
   static constexpr int NSTAGE = NST_FIT < NST_CAP ? NST_FIT : NST_CAP;
   static constexpr int OFF_B = NSTAGE * STAGE_BYTES;
   static constexpr int OFF_STG = OFF_B + B_ALLOC;
-  static constexpr int OFF_CTRL = OFF_STG + 2 * STG_BUFS * STG_BYTES;
+  static constexpr int OFF_MASK = OFF_STG + 2 * STG_BUFS * STG_BYTES;
+  static constexpr int OFF_CTRL = OFF_MASK + MASK_BYTES;
   static constexpr int SMEM_BYTES = OFF_CTRL + CTRL_BYTES + 1024;  // + alignment slack
   static_assert(NSTAGE >= BPT, "stage ring must hold a whole tile");
+  static_assert(!SEG || W == 32 || W == 64, "segmented modes use S = 32 or 64");
   static_assert(W == 16 || W == 32 || W == 64 || W == 128, "S");
   static_assert(RB >= 32, "row must hold one 32-byte MMA K step");
   static_assert(SMEM_BYTES <= kMaxSmem, "shared memory budget");
@@ -111,8 +128,10 @@ struct ScanCtrl {
   uint64_t tile_full[2];
   uint64_t slot_empty[2][16];
   uint64_t drain;
-  uint64_t agg_full[8];             // summer -> epilogue: tile aggregate published
+  uint64_t agg_full[8];             // summer -> epilogue: tile aggregate published / bound index ready
   uint64_t agg_empty[8];            // epilogue -> summer: ring slot free
+  long long tile_i0[8];             // kSegBounds: first bound index >= tile start
+  int wg_vote[2][4];
   uint32_t stage_cid[32];
   uint32_t tile_cid[2];
   uint32_t tmem_base;
@@ -392,6 +411,32 @@ __device__ __forceinline__ void scan_epilogue(const ScanParams& p, const CUtenso
   if (wg_thread == 0) bulk_wait_all0();
 }
 
+// Segment-start array element (int32 or int64).
+__device__ __forceinline__ long long bound_at(const ScanParams& p, int64_t i) {
+  return p.bounds64 ? __ldg(static_cast<const long long*>(p.bounds) + i)
+                    : (long long)__ldg(static_cast<const int*>(p.bounds) + i);
+}
+
+// First index i in [0, nbounds] with bounds[i] >= target (warp-cooperative,
+// 32-way search: four rounds for a million entries).  Run by one full warp.
+__device__ __forceinline__ long long warp_lower_bound(const ScanParams& p, long long target) {
+  const int lane = threadIdx.x & 31;
+  long long lo = 0, hi = p.nbounds;
+  while (hi - lo > 32) {
+    const long long step = (hi - lo + 31) / 32;
+    const long long pos = lo + lane * step;
+    const bool below = pos < hi && bound_at(p, pos) < target;
+    const int c = __popc(__ballot_sync(0xffffffffu, below));
+    const long long nlo = c == 0 ? lo : lo + (c - 1) * step + 1;
+    const long long nhi = (c == 32) ? hi : min(hi, lo + (long long)c * step);
+    lo = nlo;
+    hi = nhi;
+  }
+  const long long pos = lo + lane;
+  const bool below = pos < hi && bound_at(p, pos) < target;
+  return lo + __popc(__ballot_sync(0xffffffffu, below));
+}
+
 // Summer warp: sums every tile straight from the TMA-filled SMEM stages (rows
 // past the input are skipped, the partial last row is read from global) and
 // publishes the tile aggregate at once, then hands (tile, aggregate) to the
@@ -402,7 +447,7 @@ __device__ __forceinline__ void scan_epilogue(const ScanParams& p, const CUtenso
 template <typename InT, int W, int MODE>
 __device__ __forceinline__ void scan_summer(const ScanParams& p, uint8_t* smem, ScanCtrl* ctl, uint32_t epoch,
                                                 const WaitCtx& wc) {
-  using C = ScanCfg<InT, W>;
+  using C = ScanCfg<InT, W, is_seg(MODE)>;
   constexpr bool IS_INT = C::IS_INT;
   constexpr int BPT = C::BPT;
   using V = typename std::conditional<IS_INT, long long, double>::type;
@@ -455,6 +500,21 @@ __device__ __forceinline__ void scan_summer(const ScanParams& p, uint8_t* smem, 
       if (lane == 0) mbar_arrive(&ctl->empty[s]);  // this consumer is done with the stage
     }
     if (stop) break;
+    if constexpr (MODE == kSegBounds) {
+      // first bound index of the tile, found ahead of the epilogue
+      const long long i0 = warp_lower_bound(p, (long long)tid * C::TILE_ELEMS);
+      int ok = 1;
+      if (lane == 0) {
+        const int m = i & 7;
+        if (i >= 8) ok = mbar_wait(&ctl->agg_empty[m], ((i >> 3) & 1u) ^ 1u, wc, 8, i) ? 1 : 0;
+        if (ok) {
+          ctl->tile_i0[m] = i0;
+          mbar_arrive(&ctl->agg_full[m]);
+        }
+      }
+      ok = __shfl_sync(0xffffffffu, ok, 0);
+      if (!ok) break;
+    }
     if constexpr (MODE == kScanFull) {
       const int64_t tile_row0 = (int64_t)tid * BPT * 128;
       if (lane == 0 && p.tail > 0 && p.full_rows >= tile_row0 && p.full_rows < tile_row0 + BPT * 128) {
@@ -483,11 +543,321 @@ __device__ __forceinline__ void scan_summer(const ScanParams& p, uint8_t* smem, 
   }
 }
 
+// ---------------------------------------------------------------------------
+// Segmented modes.
+
+// Warpgroup-wide count of `pred` (two named barriers).
+__device__ __forceinline__ int wg_count(bool pred, int* votes, int lane, int q, uint32_t bar_id) {
+  const int c = __popc(__ballot_sync(0xffffffffu, pred));
+  if (lane == 0) votes[q] = c;
+  named_bar_sync(bar_id, 128);
+  const int t = votes[0] + votes[1] + votes[2] + votes[3];
+  named_bar_sync(bar_id, 128);
+  return t;
+}
+
+// Start mask of the row beginning at element a (bit j: a segment starts at
+// a + j) for the flag and periodic modes.  Rows past the input have none.
+template <int W, int MODE>
+__device__ __forceinline__ unsigned long long row_start_mask(const ScanParams& p, int64_t a) {
+  if (a >= p.n) return 0ull;
+  unsigned long long m = 0;
+  if constexpr (MODE == kSegPeriodic) {
+    const int64_t L = p.period;
+    for (int64_t pp = ((a + L - 1) / L) * L; pp < a + W; pp += L) m |= 1ull << (pp - a);
+    return m;
+  } else {
+    const int8_t* f = p.flags + a;
+    if (a + W <= p.n) {
+      const uint4* fv = reinterpret_cast<const uint4*>(f);
+#pragma unroll
+      for (int v = 0; v < W / 16; ++v) {
+        const uint4 w = __ldg(fv + v);
+        const unsigned long long bits = (unsigned long long)(sel4(w.x) | (sel4(w.y) << 4) | (sel4(w.z) << 8) |
+                                                             (sel4(w.w) << 12));
+        m |= bits << (16 * v);
+      }
+    } else {
+      for (int j = 0; j < W && a + j < p.n; ++j)
+        if (f[j] != 0) m |= 1ull << j;
+    }
+    if constexpr (MODE == kSegEnds) {
+      // a segment starts right after every end flag
+      m = (m << 1) | ((a > 0 && p.flags[a - 1] != 0) ? 1ull : 0ull);
+      if constexpr (W < 64) m &= (1ull << W) - 1ull;
+    }
+    return m;
+  }
+}
+
+__device__ __forceinline__ uint32_t stage_lookup(const uint8_t* stg, int64_t pos_local, int W, int OBW, int OSW) {
+  const int row = (int)(pos_local / W), col = (int)(pos_local % W);
+  const int box = col / OBW, cin = col % OBW;
+  return *reinterpret_cast<const uint32_t*>(stg + box * (128 * OSW) + swz(row * OSW + cin * 4, OSW));
+}
+
+template <typename InT, int W, int MODE>
+__device__ __forceinline__ void seg_epilogue(const ScanParams& p, const CUtensorMap& out_map, uint8_t* smem,
+                                             ScanCtrl* ctl, uint32_t tmem_base, uint32_t epoch,
+                                             const WaitCtx& wc) {
+  using C = ScanCfg<InT, W, true>;
+  constexpr bool IS_INT = C::IS_INT;
+  constexpr int BPT = C::BPT;
+  using V = typename std::conditional<IS_INT, long long, double>::type;
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  const int g = (warp - 2) >> 2;
+  const int q = warp & 3;
+  const int r = q * 32 + lane;
+  const int wg_thread = threadIdx.x - 64 - g * 128;
+  const uint32_t bar_id = 1 + g;
+  uint8_t* stg_base = smem + C::OFF_STG + g * C::STG_BUFS * C::STG_BYTES;
+  unsigned long long* smask = reinterpret_cast<unsigned long long*>(smem + C::OFF_MASK) + g * BPT * 128;
+  int* votes = ctl->wg_vote[g];
+  const bool sums_out = (MODE == kSegBounds) && p.out_sums;
+  const bool prof = p.phase_ns != nullptr && wg_thread == 0;
+  uint64_t t_mark = prof ? globaltimer() : 0;
+  uint32_t nfill = 0;
+
+  for (uint32_t i = g;; i += 2) {
+    const uint32_t u = i >> 1;
+    int ok = 1;
+    if (lane == 0) ok = mbar_wait(&ctl->tile_full[g], u & 1u, wc, 5, i) ? 1 : 0;
+    ok = __shfl_sync(0xffffffffu, ok, 0);
+    if (lane == 0) ctl->wait_ok[g][q] = ok;
+    named_bar_sync(bar_id, 128);
+    const int all_ok = ctl->wait_ok[g][0] & ctl->wait_ok[g][1] & ctl->wait_ok[g][2] & ctl->wait_ok[g][3];
+    const uint32_t tid = *(volatile uint32_t*)&ctl->tile_cid[g];
+    if (!all_ok || tid == kSentinel) break;
+    if (prof) { const uint64_t t = globaltimer(); phase_add(p, 0, t - t_mark); phase_add(p, 7, 1); t_mark = t; }
+    tc_fence_after();
+    const uint32_t tm = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(g * 256);
+    const int64_t row_tile0 = (int64_t)tid * BPT * 128;
+    const int64_t tile_e0 = row_tile0 * W;
+    const int64_t tile_e1 = min(tile_e0 + (int64_t)C::TILE_ELEMS, p.n);
+
+    // ---- start masks of every row of the tile ----
+    long long cur = 0;  // bound cursor (kSegBounds)
+    if constexpr (MODE == kSegBounds) {
+      const int m = i & 7;
+      if (wg_thread == 0) mbar_wait(&ctl->agg_full[m], (i >> 3) & 1u, wc, 6, i);
+#pragma unroll
+      for (int j = 0; j < BPT; ++j) smask[j * 128 + r] = 0ull;
+      named_bar_sync(bar_id, 128);
+      cur = *(volatile long long*)&ctl->tile_i0[m];
+      for (long long base = cur;; base += 128) {
+        const long long idx = base + wg_thread;
+        const long long b = idx < p.nbounds ? bound_at(p, idx) : LLONG_MAX;
+        const bool in = b < tile_e1;
+        if (in && b >= tile_e0) {
+          const long long off = b - tile_e0;
+          const int row = (int)(off / W);
+          atomicOr(&smask[row], 1ull << (off % W));
+        }
+        if (wg_count(in, votes, lane, q, bar_id) < 128) break;
+      }
+      if (wg_thread == 0) mbar_arrive(&ctl->agg_empty[m]);  // every thread has read tile_i0
+    } else {
+#pragma unroll
+      for (int j = 0; j < BPT; ++j) smask[j * 128 + r] = row_start_mask<W, MODE>(p, (row_tile0 + j * 128 + r) * W);
+    }
+
+    // ---- (A) segmented row aggregates -> row offsets, tile aggregate ----
+    V rowex[BPT];
+    int exf[BPT];
+    {
+      uint32_t tb[BPT];
+      int fl[BPT];
+#pragma unroll
+      for (int j = 0; j < BPT; ++j) {
+        const int64_t grow = row_tile0 + j * 128 + r;
+        const bool is_tail = grow == p.full_rows && p.tail > 0;
+        const bool live = grow < p.full_rows || is_tail;
+        const unsigned long long mk = smask[j * 128 + r];
+        float accf = 0.f, basef = 0.f, prevf = 0.f;
+        int acci = 0, basei = 0, previ = 0;
+        bool seen = false;
+#pragma unroll
+        for (int c = 0; c < W / 16; ++c) {
+          uint32_t v[16];
+          tmem_ld16(tm + (uint32_t)(j * W + c * 16), v);
+          tmem_wait_ld();
+          if (is_tail) tail_chunk<InT, W>(p, c * 16, v, accf, acci);
+#pragma unroll
+          for (int e = 0; e < 16; ++e) {
+            const int col = c * 16 + e;
+            if ((mk >> col) & 1ull) {
+              basef = prevf;
+              basei = previ;
+              seen = true;
+            }
+            prevf = __uint_as_float(v[e]);
+            previ = (int)v[e];
+          }
+        }
+        // z[W-1] is prevf / previ; aggregate after the last start
+        if constexpr (IS_INT) tb[j] = live ? (uint32_t)(previ - (seen ? basei : 0)) : 0u;
+        else tb[j] = live ? __float_as_uint(prevf - (seen ? basef : 0.f)) : 0u;
+        fl[j] = (live && mk != 0ull) ? 1 : 0;
+      }
+      int rowf[BPT];
+#pragma unroll
+      for (int j = 0; j < BPT; ++j) {
+        V ti = IS_INT ? (V)(int)tb[j] : (V)__uint_as_float(tb[j]);
+        int fi = fl[j];
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+          const V tp = __shfl_up_sync(0xffffffffu, ti, d);
+          const int fp = __shfl_up_sync(0xffffffffu, fi, d);
+          if (lane >= d) seg_combine(fi, ti, fp, tp);
+        }
+        V te = __shfl_up_sync(0xffffffffu, ti, 1);
+        int fe = __shfl_up_sync(0xffffffffu, fi, 1);
+        if (lane == 0) { te = V(0); fe = 0; }
+        rowex[j] = te;
+        rowf[j] = fe;
+        if (lane == 31) {
+          ctl->wt[g][j][q] = v_bits<V>(ti);
+          ctl->wt_flag[g][j][q] = (uint8_t)fi;
+        }
+      }
+      named_bar_sync(bar_id, 128);
+      V run = V(0);
+      int runf = 0;
+#pragma unroll
+      for (int j = 0; j < BPT; ++j) {
+        V wpre = V(0), bsum = V(0);
+        int wf = 0, bf = 0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const V wv = v_from_bits<V>(ctl->wt[g][j][k]);
+          const int wfl = ctl->wt_flag[g][j][k];
+          if (k < q) { if (wfl) { wpre = wv; wf = 1; } else { wpre += wv; } }
+          if (wfl) { bsum = wv; bf = 1; } else { bsum += wv; }
+        }
+        V ex = rowex[j];
+        int f = rowf[j];
+        if (!f) { ex = wpre + ex; f = wf; }
+        if (!f) { ex = run + ex; f = runf; }
+        rowex[j] = ex;
+        exf[j] = f;
+        if (bf) { run = bsum; runf = 1; } else { run += bsum; }
+      }
+      if (prof) { const uint64_t t = globaltimer(); phase_add(p, 1, t - t_mark); t_mark = t; }
+      // publish the (segmented) tile aggregate, then look back; a tile that
+      // holds a segment start ends every look-back that reaches it
+      if (wg_thread == 0) publish_aggregate<V>((int64_t)tid, run, runf, V(0), p.descs, epoch);
+      const V pre = wg_lookback<V>((int64_t)tid, run, V(0), p.descs, epoch, wc, &ctl->lb[g], wg_thread, bar_id,
+                                   runf);
+#pragma unroll
+      for (int j = 0; j < BPT; ++j)
+        if (!exf[j]) rowex[j] = pre + rowex[j];
+      if (prof) { const uint64_t t = globaltimer(); phase_add(p, 2, t - t_mark); t_mark = t; }
+    }
+
+    // ---- (C) drain: in-row segment fix-ups, carry, staging, output ----
+#pragma unroll 1
+    for (int j = 0; j < BPT; ++j) {
+      const int64_t brow0 = row_tile0 + j * 128;
+      const int64_t grow = brow0 + r;
+      const bool is_tail = (grow == p.full_rows) && p.tail > 0;
+      const unsigned long long mk = smask[j * 128 + r];
+      float accf = 0.f, basef = 0.f, prevf = 0.f;
+      int acci = 0, basei = 0, previ = 0;
+      bool seen = false;
+      const float cf = IS_INT ? 0.f : (float)rowex[j];
+      const uint32_t ci = IS_INT ? (uint32_t)(long long)rowex[j] : 0u;
+      uint8_t* stg = stg_base + (nfill % C::STG_BUFS) * C::STG_BYTES;
+      if (wg_thread == 0) {
+        if (C::STG_BUFS == 2) bulk_wait_read1(); else bulk_wait_read0();
+      }
+      named_bar_sync(bar_id, 128);
+      uint32_t v[W];
+#pragma unroll
+      for (int c = 0; c < W / 16; ++c)
+        tmem_ld16(tm + (uint32_t)(j * W + c * 16), *reinterpret_cast<uint32_t(*)[16]>(&v[c * 16]));
+      tmem_wait_ld();
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&ctl->slot_empty[g][j]);
+      if (is_tail) {
+#pragma unroll
+        for (int c = 0; c < W / 16; ++c)
+          tail_chunk<InT, W>(p, c * 16, *reinterpret_cast<uint32_t(*)[16]>(&v[c * 16]), accf, acci);
+      }
+#pragma unroll
+      for (int e4 = 0; e4 < W / 4; ++e4) {
+        uint32_t o[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const int col = e4 * 4 + e;
+          if ((mk >> col) & 1ull) {
+            basef = prevf;
+            basei = previ;
+            seen = true;
+          }
+          const uint32_t z = v[col];
+          if constexpr (IS_INT) o[e] = seen ? (uint32_t)((int)z - basei) : z + ci;
+          else o[e] = __float_as_uint(seen ? __uint_as_float(z) - basef : __uint_as_float(z) + cf);
+          prevf = __uint_as_float(z);
+          previ = (int)z;
+        }
+        const int cc = e4 * 4;
+        const int box = cc / C::OBW, cin = cc % C::OBW;
+        *(uint4*)(stg + box * (128 * C::OSW) + swz(r * C::OSW + cin * 4, C::OSW)) = make_uint4(o[0], o[1], o[2], o[3]);
+        if (is_tail && !sums_out) {
+          uint32_t* zt = (uint32_t*)p.z + p.full_rows * (int64_t)W + cc;
+#pragma unroll
+          for (int e = 0; e < 4; ++e)
+            if (cc + e < p.tail) zt[e] = o[e];
+        }
+      }
+      fence_proxy_async_smem();
+      named_bar_sync(bar_id, 128);
+      if (!sums_out) {
+        if (wg_thread == 0) {
+          if (p.has_map && brow0 < p.full_rows) {
+#pragma unroll
+            for (int b = 0; b < W / C::OBW; ++b)
+              tma_store_2d(&out_map, b * C::OBW, (int32_t)brow0, stg + b * (128 * C::OSW));
+          }
+          bulk_commit();
+        }
+      } else {
+        // one output per segment whose last element lies in this block:
+        // out[k] = y[bounds[k+1] - 1] (0 for an empty segment)
+        const int64_t be0 = brow0 * W;
+        const int64_t be1 = min(be0 + 128 * (int64_t)W, p.n);
+        for (long long base = cur;; base += 128) {
+          const long long idx = base + wg_thread;
+          const long long b = idx < p.nbounds ? bound_at(p, idx) : LLONG_MAX;
+          const bool in = b <= be1;
+          if (in && idx >= 1 && (b > be0 || (be0 == 0 && b == 0))) {
+            const long long bp = bound_at(p, idx - 1);
+            uint32_t val = 0u;
+            if (b > bp && b > be0) val = stage_lookup(stg, b - 1 - be0, W, C::OBW, C::OSW);
+            static_cast<uint32_t*>(p.seg_out)[idx - 1] = val;
+          }
+          const int nin = wg_count(in, votes, lane, q, bar_id);
+          if (nin < 128) {
+            cur = base + nin;
+            break;
+          }
+        }
+        if (wg_thread == 0) bulk_commit();  // keeps the staging double-buffer accounting uniform
+      }
+      ++nfill;
+    }
+    if (prof) { const uint64_t t = globaltimer(); phase_add(p, 3, t - t_mark); t_mark = t; }
+  }
+  if (wg_thread == 0) bulk_wait_all0();
+}
+
 template <typename InT, int W, int MODE>
 __global__ void __launch_bounds__(kThreads, 1)
     scan_tc_kernel(const __grid_constant__ CUtensorMap in_map, const __grid_constant__ CUtensorMap out_map,
                    const ScanParams p) {
-  using C = ScanCfg<InT, W>;
+  using C = ScanCfg<InT, W, is_seg(MODE)>;
   constexpr bool IS_INT = C::IS_INT;
   constexpr int BPT = C::BPT;
   using V = typename std::conditional<IS_INT, long long, double>::type;
@@ -637,7 +1007,8 @@ __global__ void __launch_bounds__(kThreads, 1)
       mbar_drain(&ctl->drain, 0, p.timeout_ns);
     }
   } else if (warp < 10) {
-    scan_epilogue<InT, W, MODE>(p, out_map, smem, ctl, tmem_base, epoch, wc);
+    if constexpr (is_seg(MODE)) seg_epilogue<InT, W, MODE>(p, out_map, smem, ctl, tmem_base, epoch, wc);
+    else scan_epilogue<InT, W, MODE>(p, out_map, smem, ctl, tmem_base, epoch, wc);
   } else {
     scan_summer<InT, W, MODE>(p, smem, ctl, epoch, wc);
   }

@@ -392,6 +392,158 @@ def run_complete_blocks(x, sums, tile_length):
     return z
 
 
+# ---------------------------------------------------------------------------
+# segmented operators (src/torch/torch_seg_ops.h)
+
+def _seg_x(x, where):
+    x = _cuda_input(x)
+    if x.dtype not in (torch.float16, torch.int8):
+        raise TypeError(f"{where}: x must be float16 or int8, got {x.dtype}")
+    return x
+
+
+def _flags_input(f, n, device, where):
+    f = _cuda_input(f, "f")
+    if f.device != device:
+        raise ValueError(f"{where}: f must be on the device of x")
+    if f.dtype in (torch.bool, torch.uint8):
+        f = f.view(torch.int8)
+    if f.dtype != torch.int8:
+        raise TypeError(f"{where}: f must be int8, got {f.dtype}")
+    if f.numel() != n:
+        raise ValueError(f"{where}: f has {f.numel()} elements, x has {n}")
+    return f
+
+
+def _seg_scan_flags(x, f, S, ends, where):
+    n = x.numel()
+    z = torch.empty(n, dtype=_scan_out_dtype(x.dtype), device=x.device)
+    if n == 0:
+        return z
+    S = _pick_S(S, x.dtype, n)
+    ws, wsb = workspace(x.device, _lib.lib.tcu_workspace_bytes(n, S))
+    st = _lib.lib.tcu_seg_scan(x.data_ptr(), _lib.DTYPE_CODE[x.dtype], n, S, f.data_ptr(), int(ends), z.data_ptr(),
+                               ws, wsb, stream_ptr(x.device))
+    check(st, where)
+    _after(x)
+    return z
+
+
+def run_seg_scan(x, f, S):
+    """Segmented scan; f[i] != 0 starts a segment at i (reference:
+    src/torch/torch_seg_ops.h:165-193, single-core there).  One multi-CTA
+    tensor-core launch; float16 -> float32 (int8 -> int32 as an extension)."""
+    x = _seg_x(x, "run_seg_scan")
+    f = _flags_input(f, x.numel(), x.device, "run_seg_scan")
+    return _seg_scan_flags(x, f, S, False, "run_seg_scan")
+
+
+def run_seg_sum(x, f, S):
+    """Segmented sums; f[i] != 0 ENDS a segment at i, one output per end flag,
+    elements after the last end are dropped (reference:
+    src/torch/torch_seg_ops.h:85-107, semantics of tests/test_segmented_sum.py).
+
+    The reference scans, compresses the scan at the flags and takes
+    differences; here a segmented tensor-core scan yields each segment's sum
+    at its end directly (no cancellation between large prefixes) and the
+    single-pass compaction picks the ends."""
+    x = _seg_x(x, "run_seg_sum")
+    f = _flags_input(f, x.numel(), x.device, "run_seg_sum")
+    k = int(_count(f).item())
+    seg = _seg_scan_flags(x, f, S, True, "run_seg_sum")
+    return _compress(seg, f, k, where="run_seg_sum")[0]
+
+
+def _bounds_input(indptr, device, where):
+    if not isinstance(indptr, torch.Tensor):
+        raise TypeError(f"{where}: indptr must be a tensor")
+    indptr = indptr.to(device)
+    if hasattr(torch, "uint32") and indptr.dtype == torch.uint32:
+        indptr = indptr.view(torch.int32)
+    if indptr.dtype not in (torch.int32, torch.int64):
+        raise TypeError(f"{where}: indptr must be int32, uint32 or int64, got {indptr.dtype}")
+    return indptr.contiguous()
+
+
+def _seg_sum_bounds(x, bounds, S, where):
+    x = _seg_x(x, where)
+    bounds = _bounds_input(bounds, x.device, where)
+    nb = bounds.numel()
+    out = torch.empty(max(nb - 1, 0), dtype=_scan_out_dtype(x.dtype), device=x.device)
+    if nb < 2:
+        return out
+    n = x.numel()
+    S = _pick_S(S, x.dtype, n)
+    ws, wsb = workspace(x.device, _lib.lib.tcu_workspace_bytes(n, S))
+    st = _lib.lib.tcu_seg_bounds(x.data_ptr(), _lib.DTYPE_CODE[x.dtype], n, S, bounds.data_ptr(),
+                                 _lib.DTYPE_CODE[bounds.dtype], nb, 1, out.data_ptr(), ws, wsb, stream_ptr(x.device))
+    check(st, where)
+    _after(x)
+    return out
+
+
+def run_seg_sum_multi_core(x, indptr, s, segm_offsets=None):
+    """out[r] = sum x[indptr[r]:indptr[r+1]] for a CSR indptr of R+1 entries
+    (reference: src/torch/torch_seg_ops.h:333-426).  float16 -> float32,
+    int8 -> int32 (exact).  Empty segments give 0.  ``segm_offsets`` is the
+    reference's per-core segment-range hint; segment boundaries are located
+    on the device here (a per-tile search of indptr), so it is accepted for
+    signature compatibility and not read."""
+    return _seg_sum_bounds(x, indptr, s, "run_seg_sum_multi_core")
+
+
+def run_seg_sum_single_core(x, indptr, s):
+    """Same contract as run_seg_sum_multi_core (reference:
+    src/torch/torch_seg_ops.h:211-266, one core there)."""
+    return _seg_sum_bounds(x, indptr, s, "run_seg_sum_single_core")
+
+
+def run_seg_sum_multi_cube(x, upper, lower_strict, indptr, segm_offsets=None):
+    """Indptr segmented sum with S taken from ``upper`` (reference:
+    src/torch/torch_seg_ops.h:443-522; float16 only there and here)."""
+    S = _check_tri(upper, lower_strict)
+    if x.dtype != torch.float16:
+        raise TypeError(f"run_seg_sum_multi_cube: x must be fp16, got {x.dtype}")
+    return _seg_sum_bounds(x, indptr, S, "run_seg_sum_multi_cube")
+
+
+def run_seg_sum_single_cube(x, upper, lower_strict, indptr, s):
+    """Segmented sum where ``indptr`` lists segment STARTS only (R entries, the
+    last segment runs to the end of x) -- the convention of the reference's
+    single-cube variant (src/torch/torch_seg_ops.h:278-322)."""
+    _check_tri(upper, lower_strict)
+    x = _cuda_input(x)
+    starts = _bounds_input(indptr, x.device, "run_seg_sum_single_cube")
+    bounds = torch.cat([starts, torch.tensor([x.numel()], dtype=starts.dtype, device=x.device)])
+    return _seg_sum_bounds(x, bounds, s, "run_seg_sum_single_cube")
+
+
+def run_scan_batch(x, S):
+    """Row-wise scan of a 2-D [B, L] tensor (reference: src/torch/torch_scan.h:119-175):
+    float16 -> float32.  Rows are segments of one tensor-core launch."""
+    x = _cuda_input(x)
+    if x.dim() < 1:
+        raise ValueError("run_scan_batch: x must have at least one dimension")
+    L = x.shape[-1]
+    B = x.numel() // L if L else 0
+    if x.dtype == torch.float32:
+        from tcuscan_b200 import batch
+
+        return batch.scan_rows_fp32(x.reshape(B, L))
+    if x.dtype not in (torch.float16, torch.int8):
+        raise TypeError(f"run_scan_batch: x must be float16 or float32, got {x.dtype}")
+    z = torch.empty((B, L), dtype=_scan_out_dtype(x.dtype), device=x.device)
+    if B == 0 or L == 0:
+        return z
+    S = _pick_S(S, x.dtype, B * L)
+    ws, wsb = workspace(x.device, _lib.lib.tcu_workspace_bytes(B * L, S))
+    st = _lib.lib.tcu_scan_batch(x.data_ptr(), _lib.DTYPE_CODE[x.dtype], B, L, S, z.data_ptr(), ws, wsb,
+                                 stream_ptr(x.device))
+    check(st, "run_scan_batch")
+    _after(x)
+    return z
+
+
 def run_scan_cpu(x):
     """The reference's CPU scan API (src/torch/torch_scan_cpu.h:88-107):
     float16/float32 -> float32, int8 -> int32, computed on the host.  This is
