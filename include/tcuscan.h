@@ -81,7 +81,9 @@ TCU_API tcu_status_t tcu_workspace_phase_ns(void* ws, uint64_t out[8], int clear
 /* ---- scans ---------------------------------------------------------------
  * Inclusive prefix sum z = cumsum(x) + start.  x: int8 -> z int32 (exact,
  * two's-complement wrap like torch.cumsum(dtype=int32)); x: fp16 -> z fp32
- * (FP32 tensor-core rows, FP64 carry chain).  S in {16,32,64,128} is the row
+ * (FP32 tensor-core rows, FP64 carry chain); x: fp32 -> z fp32 (each value
+ * split into bf16 hi = RN(x) and lo = RN(x - hi), two MMAs into one FP32
+ * accumulator, FP64 carry chain; S is fixed to 64).  S in {16,32,64,128} is the row
  * length of the S x S triangular tile multiplied on the tensor cores.
  * Replaces run_scan_multi_core (src/torch/torch_scan.h:184-241),
  * run_scan_multi_core_no_l2 (:253-304), run_scan_single_core (:47-110,
@@ -100,7 +102,8 @@ TCU_API tcu_status_t tcu_block_scan(const void* x, tcu_dtype_t x_dtype, int64_t 
                             size_t ws_bytes, void* stream);
 
 /* ---- segmented scans (tensor cores) ---------------------------------------
- * Segmented inclusive scan of x (int8 -> int32 exact, fp16 -> fp32).
+ * Segmented inclusive scan of x (int8 -> int32 exact, fp16 -> fp32, fp32 ->
+ * fp32 via split-precision bf16 hi + lo operands).
  * flags_are_ends = 0: flags[i] != 0 starts a segment at i (run_seg_scan,
  * src/torch/torch_seg_ops.h:165-193); 1: flags[i] != 0 ends a segment at i,
  * the building block of run_seg_sum (:85-107).  S in {16,32,64,128} (tiles of
@@ -116,7 +119,20 @@ TCU_API tcu_status_t tcu_seg_scan(const void* x, tcu_dtype_t x_dtype, int64_t n,
 TCU_API tcu_status_t tcu_seg_bounds(const void* x, tcu_dtype_t x_dtype, int64_t n, int S, const void* bounds,
                                     tcu_dtype_t bounds_dtype, int64_t nbounds, int out_sums, void* out, void* ws,
                                     size_t ws_bytes, void* stream);
-/* Row-wise scan of a row-major [batch, len] matrix (int8 / fp16).
+/* CSR SpMV y = A x with y fp32: products vals[i] * x[cols[i]] formed in fp32
+ * (fp16 products exact) into the caller's prod_tmp (nnz floats, 16-byte
+ * aligned), then indptr segment sums on the tensor cores (split-precision
+ * bf16 hi + lo, FP64 carries across tiles).  indptr has rows + 1 entries
+ * (int32 or int64).  Replaces run_spmv_v2 (src/torch/torch_spmv.h:112-209),
+ * run_spmv_v2_multi_cube (:235-302), run_spmv (:63-94) and
+ * run_spmv_multi_cube (:32-46).                                           */
+TCU_API tcu_status_t tcu_spmv_csr(const void* vals, tcu_dtype_t dtype, const void* indptr, tcu_dtype_t indptr_dtype,
+                                  int64_t rows, const int32_t* cols, int64_t nnz, const void* x, int64_t x_len, int S,
+                                  float* y, float* prod_tmp, void* ws, size_t ws_bytes, void* stream);
+/* The product step of tcu_spmv_csr on its own (fp16 / fp32 inputs). */
+TCU_API tcu_status_t tcu_spmv_products(const void* values, tcu_dtype_t dtype, const int32_t* cols, int64_t nnz,
+                                       const void* x, int64_t x_len, float* prod, void* ws, void* stream);
+/* Row-wise scan of a row-major [batch, len] matrix (int8 / fp16 / fp32).
  * Replaces run_scan_batch (src/torch/torch_scan.h:119-175).               */
 TCU_API tcu_status_t tcu_scan_batch(const void* x, tcu_dtype_t x_dtype, int64_t batch, int64_t len, int S, void* z,
                                     void* ws, size_t ws_bytes, void* stream);

@@ -141,8 +141,10 @@ static tcu_status_t launch_scan_tc(const void* x, int64_t n, void* z, double sta
   std::memset(&out_map, 0, sizeof(out_map));
   p.has_map = p.full_rows > 0;
   if (p.full_rows > 0) {
-    const CUtensorMapDataType idt = C::IS_INT ? CU_TENSOR_MAP_DATA_TYPE_UINT8 : CU_TENSOR_MAP_DATA_TYPE_UINT16;
-    tcu_status_t s = make_map_2d(&in_map, x, idt, C::ELEM, W, (uint64_t)p.full_rows, C::SW / C::ELEM, 128);
+    const CUtensorMapDataType idt = C::IN_BYTES == 1 ? CU_TENSOR_MAP_DATA_TYPE_UINT8
+                                    : (C::IN_BYTES == 2 ? CU_TENSOR_MAP_DATA_TYPE_UINT16 : CU_TENSOR_MAP_DATA_TYPE_UINT32);
+    tcu_status_t s =
+        make_map_2d(&in_map, x, idt, C::IN_BYTES, W, (uint64_t)p.full_rows, C::IN_SW / C::IN_BYTES, 128);
     if (s != TCU_OK) return s;
     if (z != nullptr) {
       s = make_map_2d(&out_map, z, CU_TENSOR_MAP_DATA_TYPE_UINT32, 4, W, (uint64_t)p.full_rows, C::OBW, 128);
@@ -177,6 +179,10 @@ static tcu_status_t dispatch_scan(const void* x, tcu_dtype_t dt, int64_t n, int 
       default: return TCU_ERR_ARG;
     }
   }
+  if (dt == TCU_FLOAT32) {  // split-precision bf16 hi + lo operands, 64-column rows
+    if (MODE != kScanFull) return TCU_ERR_DTYPE;
+    return launch_scan_tc<float, 64, kScanFull>(x, n, z, start, 0, seg_rows, ws, ws_bytes, st);
+  }
   if (dt == TCU_FLOAT16) {
     switch (S) {
       case 16: return launch_scan_tc<__half, 16, MODE>(x, n, z, start, 0, seg_rows, ws, ws_bytes, st);
@@ -201,6 +207,7 @@ static tcu_status_t dispatch_seg(const void* x, tcu_dtype_t dt, int64_t n, int S
     if (W == 32) return launch_scan_tc<__half, 32, MODE>(x, n, z, 0.0, 0, 0, ws, ws_bytes, st, sa);
     return launch_scan_tc<__half, 64, MODE>(x, n, z, 0.0, 0, 0, ws, ws_bytes, st, sa);
   }
+  if (dt == TCU_FLOAT32) return launch_scan_tc<float, 64, MODE>(x, n, z, 0.0, 0, 0, ws, ws_bytes, st, sa);
   return TCU_ERR_DTYPE;
 }
 
@@ -330,6 +337,18 @@ tcu_status_t tcu_seg_bounds(const void* x, tcu_dtype_t x_dtype, int64_t n, int S
   sa.out_sums = out_sums ? 1 : 0;
   sa.seg_out = out_sums ? out : nullptr;
   return dispatch_seg<kSegBounds>(x, x_dtype, n, S, out_sums ? nullptr : out, sa, ws, ws_bytes, st);
+}
+
+tcu_status_t tcu_spmv_csr(const void* vals, tcu_dtype_t dtype, const void* indptr, tcu_dtype_t indptr_dtype,
+                          int64_t rows, const int32_t* cols, int64_t nnz, const void* x, int64_t x_len, int S, float* y,
+                          float* prod_tmp, void* ws, size_t ws_bytes, void* stream) {
+  if (rows < 0 || nnz < 0) return TCU_ERR_ARG;
+  if (rows == 0) return TCU_OK;
+  if (!y || !indptr || (nnz > 0 && (!prod_tmp || !vals || !cols || !x))) return TCU_ERR_ARG;
+  if (nnz > 0 && !aligned16(prod_tmp)) return TCU_ERR_ALIGN;
+  tcu_status_t s = tcu_spmv_products(vals, dtype, cols, nnz, x, x_len, prod_tmp, ws, stream);
+  if (s != TCU_OK) return s;
+  return tcu_seg_bounds(prod_tmp, TCU_FLOAT32, nnz, S, indptr, indptr_dtype, rows + 1, 1, y, ws, ws_bytes, stream);
 }
 
 tcu_status_t tcu_scan_batch(const void* x, tcu_dtype_t x_dtype, int64_t batch, int64_t len, int S, void* z, void* ws,

@@ -81,13 +81,19 @@ constexpr int kMaxSmem = 232448;
 
 template <typename InT, int W, bool SEG = false>
 struct ScanCfg {
-  static constexpr int ELEM = (int)sizeof(InT);
-  static constexpr bool IS_INT = (ELEM == 1);
-  static constexpr int RB = W * ELEM;                 // row bytes
-  static constexpr int SW = RB < 128 ? RB : 128;      // swizzle span
+  static constexpr int IN_BYTES = (int)sizeof(InT);   // input element bytes
+  static constexpr bool IS_F32 = (IN_BYTES == 4);     // fp32: split into bf16 hi + lo operands
+  static constexpr int ELEM = IS_F32 ? 2 : IN_BYTES;  // MMA operand element bytes
+  static constexpr bool IS_INT = (IN_BYTES == 1);
+  static constexpr int RB = W * ELEM;                 // operand row bytes
+  static constexpr int SW = RB < 128 ? RB : 128;      // operand swizzle span
   static constexpr int KB = RB / SW;                  // K blocks of SW bytes
   static constexpr int KSTEPS = SW / 32;              // 32-byte MMA K steps per block
-  static constexpr int STAGE_BYTES = 128 * RB;
+  static constexpr int IN_RB = W * IN_BYTES;          // input row bytes (TMA geometry)
+  static constexpr int IN_SW = IN_RB < 128 ? IN_RB : 128;
+  static constexpr int IN_KB = IN_RB / IN_SW;
+  static constexpr int STAGE_BYTES = 128 * IN_RB;
+  static constexpr int TERM_BYTES = 128 * RB;         // fp32: hi operand at 0, lo at TERM_BYTES
   static constexpr int BPT = 256 / W;                 // blocks per tile
   static constexpr int TILE_ELEMS = 128 * 256;
   static constexpr int B_BYTES = W * RB;
@@ -100,7 +106,7 @@ struct ScanCfg {
   // holds as many blocks as fit (at least one tile, at most four); output
   // staging is double buffered unless that would leave under two tiles of
   // input stages.
-  static constexpr int CTRL_BYTES = 3072;
+  static constexpr int CTRL_BYTES = 3328;
   static constexpr int B_ALLOC = ((B_BYTES + 1023) / 1024) * 1024;
   // segmented modes keep one 64-bit start mask per row of a tile per warpgroup
   static constexpr int MASK_BYTES = SEG ? 2 * BPT * 128 * 8 : 0;
@@ -117,6 +123,7 @@ struct ScanCfg {
   static constexpr int SMEM_BYTES = OFF_CTRL + CTRL_BYTES + 1024;  // + alignment slack
   static_assert(NSTAGE >= BPT, "stage ring must hold a whole tile");
   static_assert(!SEG || W == 32 || W == 64, "segmented modes use S = 32 or 64");
+  static_assert(!IS_F32 || W == 64, "fp32 inputs use 64-column rows");
   static_assert(W == 16 || W == 32 || W == 64 || W == 128, "S");
   static_assert(RB >= 32, "row must hold one 32-byte MMA K step");
   static_assert(SMEM_BYTES <= kMaxSmem, "shared memory budget");
@@ -125,6 +132,7 @@ struct ScanCfg {
 struct ScanCtrl {
   uint64_t full[32];
   uint64_t empty[32];
+  uint64_t conv[32];                // fp32: stage converted to bf16 hi/lo operands
   uint64_t tile_full[2];
   uint64_t slot_empty[2][16];
   uint64_t drain;
@@ -142,7 +150,7 @@ struct ScanCtrl {
   uint8_t wt_flag[2][16][4];        // warp segment flags per block
   LbScratch lb[2];
 };
-static_assert(sizeof(ScanCtrl) <= 3072, "control block");
+static_assert(sizeof(ScanCtrl) <= 3328, "control block");
 
 // Value of 1 in the MMA operand encoding.
 template <typename T>
@@ -160,6 +168,8 @@ template <>
 __device__ __forceinline__ float load_elem<__half>(const __half* p) { return __half2float(*p); }
 template <>
 __device__ __forceinline__ float load_elem<__nv_bfloat16>(const __nv_bfloat16* p) { return __bfloat162float(*p); }
+template <>
+__device__ __forceinline__ float load_elem<float>(const float* p) { return *p; }
 
 // Segmented carry operator on (flag, value): (f1,v1) + (f2,v2) =
 // (f1|f2, f2 ? v2 : v1+v2).  Plain scans only ever use flag = 0.
@@ -169,12 +179,29 @@ __device__ __forceinline__ void seg_combine(int& f, V& v, int f_prev, V v_prev) 
   f |= f_prev;
 }
 
+// Split four fp32 values into bf16 hi = RN(x) and lo = RN(x - hi) (x - hi
+// is exact in fp32), packed four per uint2 in column order.
+__device__ __forceinline__ void split_bf16x4(const float4 v, uint2& hi, uint2& lo) {
+  const __nv_bfloat162 h01 = __floats2bfloat162_rn(v.x, v.y);
+  const __nv_bfloat162 h23 = __floats2bfloat162_rn(v.z, v.w);
+  const float2 f01 = __bfloat1622float2(h01), f23 = __bfloat1622float2(h23);
+  const __nv_bfloat162 l01 = __floats2bfloat162_rn(v.x - f01.x, v.y - f01.y);
+  const __nv_bfloat162 l23 = __floats2bfloat162_rn(v.z - f23.x, v.w - f23.y);
+  hi = make_uint2(*reinterpret_cast<const uint32_t*>(&h01), *reinterpret_cast<const uint32_t*>(&h23));
+  lo = make_uint2(*reinterpret_cast<const uint32_t*>(&l01), *reinterpret_cast<const uint32_t*>(&l23));
+}
+
+template <typename InT>
+struct OperandT { using T = InT; };
+template <>
+struct OperandT<float> { using T = __nv_bfloat16; };
+
 // Build the constant operand B (K-major): row n holds U[k][n] = (k <= n).
 template <typename InT, int W>
 __device__ __forceinline__ void build_upper(uint8_t* bmat) {
   using C = ScanCfg<InT, W>;
   constexpr int CPR = C::RB / 16;  // 16-byte chunks per row
-  const uint32_t one = one_bits<InT>();
+  const uint32_t one = one_bits<typename OperandT<InT>::T>();
   for (int t = threadIdx.x; t < W * CPR; t += kThreads) {
     const int nrow = t / CPR, c = t % CPR;
     const int kb = (c * 16) / C::SW, cin = c % (C::SW / 16);
@@ -461,6 +488,7 @@ __device__ __forceinline__ void scan_summer(const ScanParams& p, uint8_t* smem, 
     bool stop = false;
     uint32_t tid = 0;
     float accf = 0.f;
+    double accd = 0.0;
     int acci = 0;
     for (int j = 0; j < BPT; ++j, ++k) {
       const int s = k % C::NSTAGE;
@@ -468,9 +496,48 @@ __device__ __forceinline__ void scan_summer(const ScanParams& p, uint8_t* smem, 
       const bool ok = __all_sync(0xffffffffu, mbar_wait(&ctl->full[s], (k / C::NSTAGE) & 1u, wc, 7, i));
       if (!ok) { stop = true; break; }
       const uint32_t cid = *(volatile uint32_t*)&ctl->stage_cid[s];
-      if (cid == kSentinel) { stop = true; break; }
+      if (cid == kSentinel) {
+        // the MMA warp of an fp32 launch waits on conv[]: pass the stop on
+        if (C::IS_F32 && lane == 0) mbar_arrive(&ctl->conv[s]);
+        stop = true;
+        break;
+      }
       tid = cid;
-      if constexpr (MODE == kScanFull) {
+      if constexpr (C::IS_F32) {
+        // In-place split of the fp32 block: each 64-column row arrives as two
+        // 128-byte halves (TMA boxes at +0 and +TERM_BYTES, same swizzle); the
+        // row is rewritten as 64 bf16 hi = RN(x) in the first slot and 64 bf16
+        // lo = RN(x - hi) in the second, the two MMA operand tiles.  A row is
+        // fully read (8 lanes x 2 x 16 B) before any lane writes it.
+        uint8_t* X0 = smem + s * C::STAGE_BYTES;
+        uint8_t* X1 = X0 + C::TERM_BYTES;
+        const int rr = lane >> 3, cidx = lane & 7;
+        const int64_t row0 = ((int64_t)tid * BPT + j) * 128;
+        const int64_t vr = p.full_rows - row0;
+        const int vrows = vr <= 0 ? 0 : (vr >= 128 ? 128 : (int)vr);
+#pragma unroll 4
+        for (int it = 0; it < 32; ++it) {
+          const int row = it * 4 + rr;
+          const uint32_t off = swz(row * 128 + cidx * 16, 128);
+          const float4 a = *reinterpret_cast<const float4*>(X0 + off);
+          const float4 b = *reinterpret_cast<const float4*>(X1 + off);
+          __syncwarp();
+          if (MODE == kScanFull && row < vrows)
+            accd += (double)((a.x + a.y) + (a.z + a.w)) + (double)((b.x + b.y) + (b.z + b.w));
+          uint2 ha, la, hb, lb;
+          split_bf16x4(a, ha, la);
+          split_bf16x4(b, hb, lb);
+          const int half = (cidx & 1) * 8;
+          *reinterpret_cast<uint2*>(X0 + swz(row * 128 + (cidx >> 1) * 16, 128) + half) = ha;
+          *reinterpret_cast<uint2*>(X0 + swz(row * 128 + (4 + (cidx >> 1)) * 16, 128) + half) = hb;
+          *reinterpret_cast<uint2*>(X1 + swz(row * 128 + (cidx >> 1) * 16, 128) + half) = la;
+          *reinterpret_cast<uint2*>(X1 + swz(row * 128 + (4 + (cidx >> 1)) * 16, 128) + half) = lb;
+        }
+        fence_proxy_async_smem();  // generic-proxy writes -> tcgen05 operand reads
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&ctl->conv[s]);
+      }
+      if constexpr (MODE == kScanFull && !C::IS_F32) {
         const int64_t row0 = ((int64_t)tid * BPT + j) * 128;
         int64_t vr = p.full_rows - row0;
         const int vrows = vr <= 0 ? 0 : (vr >= 128 ? 128 : (int)vr);
@@ -528,7 +595,7 @@ __device__ __forceinline__ void scan_summer(const ScanParams& p, uint8_t* smem, 
       }
       V agg;
       if constexpr (IS_INT) agg = (V)warp_sum_any(acci);
-      else agg = warp_sum_any((double)accf);
+      else agg = warp_sum_any((double)accf + accd);
       int ok = 1;
       if (lane == 0) {
         publish_aggregate<V>((int64_t)tid, agg, 0, start, p.descs, epoch);
@@ -874,7 +941,8 @@ __global__ void __launch_bounds__(kThreads, 1)
   if (threadIdx.x == 0) {
     for (int s = 0; s < C::NSTAGE; ++s) {
       mbar_init(&ctl->full[s], 1);
-      mbar_init(&ctl->empty[s], 2);  // MMA commit + aggregator arrive
+      mbar_init(&ctl->empty[s], 2);  // MMA commit + summer/converter arrive
+      mbar_init(&ctl->conv[s], 1);
     }
     for (int m = 0; m < 8; ++m) {
       mbar_init(&ctl->agg_full[m], 1);
@@ -938,9 +1006,9 @@ __global__ void __launch_bounds__(kThreads, 1)
           if (live && p.has_map && row0 < p.full_rows) {
             mbar_arrive_expect_tx(&ctl->full[s], C::STAGE_BYTES);
 #pragma unroll
-            for (int kb = 0; kb < C::KB; ++kb)
-              tma_load_2d(smem + s * C::STAGE_BYTES + kb * (128 * C::SW), &in_map, kb * (C::SW / C::ELEM),
-                          (int32_t)row0, &ctl->full[s]);
+            for (int kb = 0; kb < C::IN_KB; ++kb)
+              tma_load_2d(smem + s * C::STAGE_BYTES + kb * (128 * C::IN_SW), &in_map,
+                          kb * (C::IN_SW / C::IN_BYTES), (int32_t)row0, &ctl->full[s]);
           } else {
             mbar_arrive(&ctl->full[s]);
           }
@@ -954,8 +1022,9 @@ __global__ void __launch_bounds__(kThreads, 1)
   } else if (warp == 1) {
     // ================= MMA issuer =================
     if (lane == 0) {
-      constexpr uint32_t IDESC = IS_INT ? umma_idesc(CF_S32, AB_S8, 128, W)
-                                        : umma_idesc(CF_F32, __is_same(InT, __nv_bfloat16) ? AB_BF16 : AB_F16, 128, W);
+      constexpr uint32_t IDESC =
+          IS_INT ? umma_idesc(CF_S32, AB_S8, 128, W)
+                 : umma_idesc(CF_F32, (__is_same(InT, __nv_bfloat16) || C::IS_F32) ? AB_BF16 : AB_F16, 128, W);
       const uint32_t b_addr = smem_u32(bmat);
       uint32_t k = 0;
       for (uint32_t i = 0;; ++i) {  // tile sequence of this CTA
@@ -964,7 +1033,12 @@ __global__ void __launch_bounds__(kThreads, 1)
         bool fail = false, sentinel = false;
         for (int j = 0; j < BPT; ++j, ++k) {
           const int s = k % C::NSTAGE;
-          if (!mbar_wait(&ctl->full[s], (k / C::NSTAGE) & 1u, wc, 2, i)) { fail = true; break; }
+          // fp32 inputs: wait until the converter has rewritten the stage as
+          // bf16 hi/lo operands (it signals the stop-marker stage too)
+          if (!mbar_wait(C::IS_F32 ? &ctl->conv[s] : &ctl->full[s], (k / C::NSTAGE) & 1u, wc, 2, i)) {
+            fail = true;
+            break;
+          }
           const uint32_t tid = *(volatile uint32_t*)&ctl->stage_cid[s];
           if (tid == kSentinel) { sentinel = true; break; }
           if (u >= 1 && !mbar_wait(&ctl->slot_empty[g][j], (u & 1u) ^ 1u, wc, 3, tid)) { fail = true; break; }
@@ -977,8 +1051,16 @@ __global__ void __launch_bounds__(kThreads, 1)
             for (int ks = 0; ks < C::KSTEPS; ++ks) {
               const uint64_t ad = umma_desc_kmajor(a_addr + kb * (128 * C::SW) + ks * 32, C::SW);
               const uint64_t bd = umma_desc_kmajor(b_addr + kb * (W * C::SW) + ks * 32, C::SW);
-              if constexpr (IS_INT) mma_i8(d_tmem, ad, bd, IDESC, (kb | ks) != 0);
-              else mma_f16(d_tmem, ad, bd, IDESC, (kb | ks) != 0);
+              if constexpr (IS_INT) {
+                mma_i8(d_tmem, ad, bd, IDESC, (kb | ks) != 0);
+              } else if constexpr (C::IS_F32) {
+                // split precision: D += hi . U, then D += lo . U (FP32 accumulate)
+                mma_f16(d_tmem, ad, bd, IDESC, (kb | ks) != 0);
+                const uint64_t adl = umma_desc_kmajor(a_addr + C::TERM_BYTES + kb * (128 * C::SW) + ks * 32, C::SW);
+                mma_f16(d_tmem, adl, bd, IDESC, 1u);
+              } else {
+                mma_f16(d_tmem, ad, bd, IDESC, (kb | ks) != 0);
+              }
             }
           }
           tc_commit(&ctl->empty[s]);

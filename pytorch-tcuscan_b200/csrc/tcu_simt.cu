@@ -13,6 +13,13 @@
 
 namespace tcu {
 
+template <typename T>
+__device__ __forceinline__ float load_elem(const T* p);
+template <>
+__device__ __forceinline__ float load_elem<__half>(const __half* p) { return __half2float(__ldg(p)); }
+template <>
+__device__ __forceinline__ float load_elem<float>(const float* p) { return __ldg(p); }
+
 // ---------------------------------------------------------------------------
 // csr_gather.  Products are formed in the values dtype exactly as torch
 // does: fp16 and fp32 products are correctly rounded once (an fp16 x fp16
@@ -94,6 +101,21 @@ __global__ void __launch_bounds__(256) csr_gather32_kernel(const float* __restri
     if ((unsigned)c < (unsigned long long)x_len) xv = x[c];
     else if (ws) record_error(ws, TCU_ERR_ARG, 200, (uint32_t)i);
     z[i] = __fmul_rn(vals[i], xv);
+  }
+}
+
+// SpMV products in fp32: p[i] = float(values[i]) * float(x[cols[i]]) (an
+// fp16 x fp16 product is exact in fp32; fp32 products are rounded once).
+template <typename T>
+__global__ void __launch_bounds__(256) spmv_products_kernel(const T* __restrict__ vals, const int* __restrict__ cols,
+                                                            const T* __restrict__ x, int64_t nnz, int64_t x_len,
+                                                            float* __restrict__ prod, WsHeader* ws) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nnz; i += (int64_t)gridDim.x * blockDim.x) {
+    const int c = __ldg(cols + i);
+    float xv = 0.f;
+    if ((unsigned)c < (unsigned long long)x_len) xv = load_elem<T>(x + c);
+    else if (ws) record_error(ws, TCU_ERR_ARG, 201, (uint32_t)i);
+    prod[i] = __fmul_rn(load_elem<T>(vals + i), xv);
   }
 }
 
@@ -301,6 +323,24 @@ tcu_status_t tcu_csr_gather(const void* values, tcu_dtype_t dtype, const int32_t
     return TCU_ERR_DTYPE;
   }
   return launched("csr_gather");
+}
+
+tcu_status_t tcu_spmv_products(const void* values, tcu_dtype_t dtype, const int32_t* cols, int64_t nnz, const void* x,
+                               int64_t x_len, float* prod, void* ws, void* stream) {
+  if (nnz < 0 || x_len < 0) return TCU_ERR_ARG;
+  if (nnz == 0) return TCU_OK;
+  if (!values || !cols || !x || !prod) return TCU_ERR_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  WsHeader* h = static_cast<WsHeader*>(ws);
+  if (dtype == TCU_FLOAT16)
+    spmv_products_kernel<__half><<<grid_for(nnz), 256, 0, st>>>((const __half*)values, cols, (const __half*)x, nnz,
+                                                                 x_len, prod, h);
+  else if (dtype == TCU_FLOAT32)
+    spmv_products_kernel<float><<<grid_for(nnz), 256, 0, st>>>((const float*)values, cols, (const float*)x, nnz,
+                                                                x_len, prod, h);
+  else
+    return TCU_ERR_DTYPE;
+  return launched("spmv_products");
 }
 
 tcu_status_t tcu_reduce_tiles(const void* x, tcu_dtype_t dtype, int64_t n, int64_t tile_len, int num_blocks, void* z,

@@ -397,8 +397,8 @@ def run_complete_blocks(x, sums, tile_length):
 
 def _seg_x(x, where):
     x = _cuda_input(x)
-    if x.dtype not in (torch.float16, torch.int8):
-        raise TypeError(f"{where}: x must be float16 or int8, got {x.dtype}")
+    if x.dtype not in (torch.float16, torch.int8, torch.float32):
+        raise TypeError(f"{where}: x must be float16, int8 or float32, got {x.dtype}")
     return x
 
 
@@ -526,11 +526,7 @@ def run_scan_batch(x, S):
         raise ValueError("run_scan_batch: x must have at least one dimension")
     L = x.shape[-1]
     B = x.numel() // L if L else 0
-    if x.dtype == torch.float32:
-        from tcuscan_b200 import batch
-
-        return batch.scan_rows_fp32(x.reshape(B, L))
-    if x.dtype not in (torch.float16, torch.int8):
+    if x.dtype not in (torch.float16, torch.int8, torch.float32):
         raise TypeError(f"run_scan_batch: x must be float16 or float32, got {x.dtype}")
     z = torch.empty((B, L), dtype=_scan_out_dtype(x.dtype), device=x.device)
     if B == 0 or L == 0:
@@ -542,6 +538,65 @@ def run_scan_batch(x, S):
     check(st, "run_scan_batch")
     _after(x)
     return z
+
+
+# ---------------------------------------------------------------------------
+# CSR SpMV (src/torch/torch_spmv.h)
+
+def _spmv(vals, indptr, cols, x, S, where):
+    if vals.dtype != x.dtype or vals.dtype not in (torch.float16, torch.float32):
+        raise TypeError(f"{where}: vals and x must both be fp16 or both be fp32, got vals={vals.dtype} x={x.dtype}")
+    vals, x = _cuda_input(vals, "vals"), _cuda_input(x)
+    cols = _cuda_input(cols, "cols")
+    if hasattr(torch, "uint32") and cols.dtype == torch.uint32:
+        cols = cols.view(torch.int32)
+    if cols.dtype != torch.int32:
+        cols = cols.to(torch.int32)
+    indptr = _bounds_input(indptr, x.device, where)
+    rows = indptr.numel() - 1
+    nnz = vals.numel()
+    if cols.numel() != nnz:
+        raise ValueError(f"{where}: cols and vals lengths differ")
+    y = torch.empty(max(rows, 0), dtype=torch.float32, device=x.device)
+    if rows <= 0:
+        return y
+    prod = torch.empty(max(nnz, 4), dtype=torch.float32, device=x.device)
+    S = _pick_S(S, torch.float32, nnz)
+    ws, wsb = workspace(x.device, _lib.lib.tcu_workspace_bytes(nnz, S))
+    st = _lib.lib.tcu_spmv_csr(vals.data_ptr(), _lib.DTYPE_CODE[vals.dtype], indptr.data_ptr(),
+                               _lib.DTYPE_CODE[indptr.dtype], rows, cols.data_ptr(), nnz, x.data_ptr(), x.numel(), S,
+                               y.data_ptr(), prod.data_ptr(), ws, wsb, stream_ptr(x.device))
+    check(st, where)
+    _after(x)
+    return y
+
+
+def run_spmv_v2(vals, indptr, cols, x, s, segm_offsets=None):
+    """y = A x for CSR (vals, indptr, cols) (reference: src/torch/torch_spmv.h:112-209).
+
+    vals and x both fp16 or both fp32; y is fp32.  Products are formed in fp32
+    (the reference rounds fp16 products to fp16 first) and summed per row by
+    the tensor-core segmented sum (split-precision bf16 hi + lo, FP64 carries
+    for rows spanning tiles).  ``segm_offsets`` is accepted for signature
+    compatibility and not read."""
+    return _spmv(vals, indptr, cols, x, s, "run_spmv_v2")
+
+
+def run_spmv(vals, indptr, cols, x, s):
+    """Same product as run_spmv_v2 (reference v1: src/torch/torch_spmv.h:63-94)."""
+    return _spmv(vals, indptr, cols, x, s, "run_spmv")
+
+
+def run_spmv_v2_multi_cube(vals, indptr, cols, x, upper, lower_strict):
+    """SpMV with S taken from ``upper`` (reference: src/torch/torch_spmv.h:235-302)."""
+    S = _check_tri(upper, lower_strict)
+    return _spmv(vals, indptr, cols, x, S, "run_spmv_v2_multi_cube")
+
+
+def run_spmv_multi_cube(vals, indptr, cols, x, upper, lower_strict):
+    """SpMV with S taken from ``upper`` (reference: src/torch/torch_spmv.h:32-46)."""
+    S = _check_tri(upper, lower_strict)
+    return _spmv(vals, indptr, cols, x, S, "run_spmv_multi_cube")
 
 
 def run_scan_cpu(x):

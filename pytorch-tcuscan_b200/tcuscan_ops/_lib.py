@@ -68,6 +68,8 @@ _sig("tcu_block_scan", _ST, _P, _I, _I64, _I, _P, _P, _SZ, _P)
 _sig("tcu_seg_scan", _ST, _P, _I, _I64, _I, _P, _I, _P, _P, _SZ, _P)
 _sig("tcu_seg_bounds", _ST, _P, _I, _I64, _I, _P, _I, _I64, _I, _P, _P, _SZ, _P)
 _sig("tcu_scan_batch", _ST, _P, _I, _I64, _I64, _I, _P, _P, _SZ, _P)
+_sig("tcu_spmv_csr", _ST, _P, _I, _P, _I, _I64, _P, _I64, _P, _I64, _I, _P, _P, _P, _SZ, _P)
+_sig("tcu_spmv_products", _ST, _P, _I, _P, _I64, _P, _I64, _P, _P, _P)
 _sig("tcu_compress", _ST, _P, _I, _P, _I64, _P, _I, _I, _P, _P, _I64, _P, _P, _SZ, _P)
 _sig("tcu_mask_count", _ST, _P, _I64, _P, _P)
 _sig("tcu_csr_gather", _ST, _P, _I, _P, _I64, _P, _I64, _P, _P, _P)
