@@ -91,6 +91,22 @@ TCU_API tcu_status_t tcu_workspace_phase_ns(void* ws, uint64_t out[8], int clear
 TCU_API tcu_status_t tcu_scan(const void* x, tcu_dtype_t x_dtype, int64_t n, int S, double start, void* z, void* ws,
                       size_t ws_bytes, void* stream);
 
+/* Inclusive scan that allocates nothing.  No counterpart in the reference.
+ * Same arguments and results as tcu_scan, minus the workspace, for callers
+ * that cannot allocate device memory where they scan (inside an allocator or
+ * memory-pool callback, under a fixed device budget owned by a host program,
+ * or on a path that must not reach cudaMalloc).  Its look-back scratch is a
+ * fixed 1 MiB array inside the library, held by every GPU that loads it
+ * until exit; so n is limited to 2,147,221,504 elements and larger n returns
+ * TCU_ERR_ARG.  The first call on a device looks the array up and zeroes it
+ * on `stream`: make that first call before any stream capture.  All calls
+ * share the array and it keeps the last call's contents, so calls that can
+ * overlap on the GPU (other streams, other threads) race -- serialise them.
+ * Device-side wait timeouts are not reported by this variant (tcu_scan with
+ * a workspace reports them through tcu_workspace_error).                   */
+TCU_API tcu_status_t tcu_scan_noalloc(const void* x, tcu_dtype_t x_dtype, int64_t n, int S, double start, void* z,
+                                      void* stream);
+
 /* Per-row scans of n_rows rows of S elements (z has n_rows*S elements).
  * Replaces run_row_scan (src/torch/torch_scan.h:312-351).                 */
 TCU_API tcu_status_t tcu_row_scan(const void* x, tcu_dtype_t x_dtype, int64_t n_rows, int S, void* z, void* ws,

@@ -372,3 +372,78 @@ tcu_status_t tcu_block_scan(const void* x, tcu_dtype_t x_dtype, int64_t n, int S
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Inclusive scan that allocates nothing.
+//
+// Some callers cannot allocate device memory at the point where they need a
+// scan: code that runs inside a custom allocator or memory-pool callback
+// (allocating there would re-enter the allocator), hosts that hand a plugin a
+// fixed device budget and forbid further allocations, and latency-critical
+// paths that must never reach cudaMalloc's implicit synchronisation.
+// tcu_scan asks its caller for a look-back workspace; this variant takes it
+// from a fixed array compiled into the library instead.
+namespace tcu {
+
+constexpr size_t kNoAllocScratchBytes = 1u << 20;  // 1 MiB per GPU that loads the library
+// The scratch holds a 128-byte header and one 16-byte look-back descriptor
+// per 32768-element tile: (1 MiB - 128) / 16 = 65528 tiles.
+constexpr int64_t kNoAllocMaxN = (int64_t)((kNoAllocScratchBytes - 128) / sizeof(TileDesc)) * 32768;
+
+// Device scratch of tcu_scan_noalloc.  In host code this name is only a
+// host-side stand-in: kernels get the device address that
+// cudaGetSymbolAddress returns for the current device.
+static __device__ __align__(256) uint8_t g_noalloc_scratch[kNoAllocScratchBytes];
+
+// Device address of the scratch on the current device.  The first call on a
+// device looks the address up and zeroes the array on `st`.
+static tcu_status_t noalloc_scratch(cudaStream_t st, void** out) {
+  static std::mutex mu;
+  static void* ptrs[64] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail(e, "tcu_scan_noalloc: cudaGetDevice");
+  if (dev < 0 || dev >= 64) return TCU_ERR_DEVICE;
+  std::lock_guard<std::mutex> lock(mu);
+  if (ptrs[dev] == nullptr) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || p == nullptr) return cuda_fail(e, "tcu_scan_noalloc: cudaGetSymbolAddress");
+    e = cudaMemsetAsync(p, 0, kNoAllocScratchBytes, st);
+    if (e != cudaSuccess) return cuda_fail(e, "tcu_scan_noalloc: zeroing the scratch");
+    ptrs[dev] = p;
+  }
+  *out = ptrs[dev];
+  return TCU_OK;
+}
+
+}  // namespace tcu
+
+extern "C" tcu_status_t tcu_scan_noalloc(const void* x, tcu_dtype_t x_dtype, int64_t n, int S, double start, void* z,
+                                         void* stream) {
+  if (n < 0) return TCU_ERR_ARG;
+  if (n > kNoAllocMaxN) {
+    snprintf(g_errmsg, sizeof(g_errmsg),
+             "tcu_scan_noalloc: n = %lld exceeds the %lld-element limit of its fixed scratch; "
+             "use tcu_scan with a workspace",
+             (long long)n, (long long)kNoAllocMaxN);
+    return TCU_ERR_ARG;
+  }
+  if (n == 0) return TCU_OK;
+  if (!x || !z) return TCU_ERR_ARG;
+  if (!aligned16(x) || !aligned16(z)) return TCU_ERR_ALIGN;
+  cudaStream_t st = (cudaStream_t)stream;
+  void* ws = nullptr;
+  tcu_status_t s = noalloc_scratch(st, &ws);
+  if (s != TCU_OK) return s;
+  // The tile counter, done counter and error words must start at zero (a
+  // launch resets its counters when it finishes; clearing them again costs
+  // nothing).  The epoch word is kept: it marks the look-back descriptors
+  // left by the previous call as stale.
+  uint8_t* h = static_cast<uint8_t*>(ws);
+  cudaError_t e = cudaMemsetAsync(h, 0, 2 * sizeof(uint32_t), st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(h + 3 * sizeof(uint32_t), 0, 3 * sizeof(uint32_t), st);
+  if (e != cudaSuccess) return cuda_fail(e, "tcu_scan_noalloc: clearing the scratch header");
+  if (x_dtype == TCU_INT8 && S == 16) S = 32;
+  return dispatch_scan<kScanFull>(x, x_dtype, n, S, z, start, 0, ws, kNoAllocScratchBytes, st);
+}
