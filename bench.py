@@ -129,6 +129,111 @@ class ClockSampler:
         }
 
 
+def _device_ms(fn, steps, warmup):
+    """Average device time per call of fn() (CUDA events on the current stream)."""
+    import torch
+
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    st = torch.cuda.current_stream()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(st)
+    for _ in range(steps):
+        fn()
+    b.record(st)
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / steps
+
+
+def measure_extras(dev, steps=10, warmup=3):
+    """The other configured workloads, device-timed (inputs resident in HBM,
+    all larger than L2): fp16 scan at 2^28, compaction at 2^28 with a
+    Bernoulli(0.3) mask, CSR SpMV on a 2^20 x 2^20 Zipf(1.6) matrix with
+    ~2^24 nnz, and 4096 uneven fp32 rows (log-uniform 256..2^20) scanned by
+    one CUDA-graph launch.  Errors are measured against FP64 on the device."""
+    import torch
+
+    import tcuscan_ops
+    from tcuscan_b200 import batch, workloads
+
+    peak, _ = measured_peak()
+    out = {}
+
+    def entry(elems, bytes_, ms, unit="elem/s", **kw):
+        gbs = bytes_ / (ms * 1e-3) / 1e9
+        d = {"value": elems / (ms * 1e-3), "unit": unit, "ms": ms, "GB/s": gbs, "hbm_frac": gbs / peak,
+             "algorithmic_bytes": bytes_}
+        d.update(kw)
+        return d
+
+    n = 1 << 28
+    # fp16 scan, 2^28 -> fp32
+    x = workloads.scan_input(n, torch.float16, dev, seed=7)
+    S16 = tcuscan_ops._pick_S(None, torch.float16, n)
+    ms = _device_ms(lambda: tcuscan_ops.run_scan_multi_core(x, S16), steps, warmup)
+    z = tcuscan_ops.run_scan_multi_core(x, S16)
+    ref = torch.cumsum(x.double(), 0)
+    err = ((z.double() - ref).abs() / ref.abs().clamp_min(1.0)).max().item()
+    out["scan_f16_2e28"] = entry(n, 6 * n, ms, S=S16, max_rel_err_vs_fp64=err)
+    del x, z, ref
+
+    # compaction, 2^28, mask Bernoulli(0.3): one single-pass kernel per step
+    mask = workloads.bernoulli_mask(n, 0.3, dev, seed=8)
+    k = int(mask.sum().item())
+    for name, dt in (("compress_f16", torch.float16), ("compress_i16", torch.int16), ("compress_f32", torch.float32)):
+        xv = torch.randint(-1000, 1000, (n,), device=dev).to(dt)
+        ms = _device_ms(lambda: tcuscan_ops.run_compress_pos(xv, mask, k, 64), steps, warmup)
+        eb = xv.element_size()
+        out[name] = entry(n, n * (eb + 1) + k * eb, ms, selected=k)
+        del xv
+    xv = torch.randn(n, device=dev).half()
+    ms = _device_ms(lambda: tcuscan_ops.run_compress_ind_no_arange(xv, mask, 64), 3, 1)
+    out["compress_ind_no_arange_f16_incl_count_sync"] = entry(n, n * 3 + k * 6, ms, selected=k)
+    del xv, mask
+
+    # CSR SpMV (products + indptr segment sums)
+    for name, dt in (("spmv_f32", torch.float32), ("spmv_f16", torch.float16)):
+        vals, indptr, cols, xs = workloads.zipf_csr(dtype=dt, device=dev, seed=9)
+        nnz, rows = vals.numel(), indptr.numel() - 1
+        ms = _device_ms(lambda: tcuscan_ops.run_spmv_v2(vals, indptr, cols, xs, 64), steps, warmup)
+        y = tcuscan_ops.run_spmv_v2(vals, indptr, cols, xs, 64)
+        try:  # FP64 reference on the device: per-row sums of the exact products
+            prod = vals.double() * xs.double()[cols.long()]
+            rowid = torch.repeat_interleave(torch.arange(rows, device=dev), (indptr[1:] - indptr[:-1]).long())
+            yr = torch.zeros(rows, dtype=torch.float64, device=dev).index_add_(0, rowid, prod)
+            err = ((y.double() - yr).abs() / yr.abs().clamp_min(1.0)).max().item()
+            del prod, rowid, yr
+        except RuntimeError as e:  # pragma: no cover - diagnostics only
+            err = f"unmeasured: {e}"[:120]
+        eb = vals.element_size()
+        bytes_ = nnz * (eb + 4) + (rows + 1) * 4 + rows * 4 + xs.numel() * eb
+        out[name] = entry(nnz, bytes_, ms, unit="nnz/s", rows=rows, nnz=nnz, max_rel_err_vs_fp64=err,
+                          kernels=2)
+        del vals, indptr, cols, xs, y
+
+    # 4096 uneven fp32 rows, one CUDA-graph launch
+    offs = workloads.uneven_rows(seed=10)
+    tot = int(offs[-1])
+    xr = torch.randn(tot, device=dev)
+    od = torch.from_numpy(offs).to(dev)
+    gph = batch.ScanRowsGraph(xr, od)
+    ms = _device_ms(gph.replay, max(3, steps // 2), 2)
+    zr = gph.replay()
+    seg_start = torch.repeat_interleave(od[:-1], (od[1:] - od[:-1]))
+    cs = torch.cumsum(xr.double(), 0)
+    base = torch.where(seg_start > 0, cs[(seg_start - 1).clamp_min(0)], torch.zeros_like(cs))
+    refr = cs - base
+    err_norm = ((zr.double() - refr).abs().max() / refr.abs().max().clamp_min(1.0)).item()
+    err_el = ((zr.double() - refr).abs() / refr.abs().clamp_min(1.0)).max().item()
+    out["batch_rows_f32_4096"] = entry(tot, tot * 8 + offs.size * 8, ms, rows=4096,
+                                       normwise_rel_err_vs_fp64=err_norm, max_rel_err_vs_fp64=err_el,
+                                       launch="one CUDA-graph replay per step")
+    del xr, zr, cs, base, refr, seg_start
+    torch.cuda.empty_cache()
+    return out
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -198,10 +303,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--op", default="scan_i8", choices=sorted(OPS))
-    ap.add_argument("--S", type=int, default=64)
+    ap.add_argument("--S", type=int, default=0, help="tile parameter (0 = autotuned default)")
     ap.add_argument("--n", type=int, default=1 << 28)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--phases", action="store_true", help="print a per-phase device-time breakdown (diagnostics)")
+    ap.add_argument("--no-extras", action="store_true", help="headline workload only")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -223,6 +329,8 @@ def main():
 
     dname, bpe, desc = OPS[args.op]
     n = args.n
+    if not args.S:
+        args.S = tcuscan_ops._pick_S(None, torch.int8 if dname == "int8" else torch.float16, n)
     g = torch.Generator(device=dev).manual_seed(1234 + rank)
     if dname == "int8":
         x = torch.randint(-8, 9, (n,), dtype=torch.int8, device=dev, generator=g)
@@ -313,6 +421,11 @@ def main():
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         e2e_ms = float(t.item())
 
+    extras = None
+    if rank == 0 and world == 1 and not args.no_extras:
+        del x_host, z_host, x_dev
+        extras = measure_extras(dev)
+
     cpu_base = None
     if rank == 0 and world == 1 and not args.no_cpu:
         sample = min(n, 1 << 26)
@@ -355,6 +468,7 @@ def main():
                 "ms_per_step": e2e_ms / e2e_steps},
         "clocks": clocks,
         "gpu_launches": args.steps,
+        "extras": extras,
     }
     print(json.dumps(line), flush=True)
     return 0
