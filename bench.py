@@ -234,6 +234,110 @@ def measure_extras(dev, steps=10, warmup=3):
     return out
 
 
+def measure_serving(dev, count=20000, seed=11, sample=240):
+    """The served request stream (20000 requests: 50% scan / 30% indptr
+    seg_sum / 20% compress; 40% int8 / 40% float16 / 20% float32; sizes
+    log-uniform in [2^10, 2^24]; geometric(mean 64) segments; 24 GB admission
+    budget) through the serving loop and through a loop of single drop-in
+    calls.  Both arms read the same request data from HBM; completions are
+    read on the device clock (CUDA events against a start event).
+    Throughput: every request available at t = 0.  Latency: Poisson arrivals
+    at half the served throughput, p50/p99 of completion - arrival.
+    Accuracy: a sample of requests served in the mix is compared with the
+    single calls (integer results bit-exact, floating max relative diff)."""
+    import numpy as np
+    import torch
+
+    from tcuscan_b200 import serve, workloads
+
+    wl = workloads.ServedStream(count, dev, seed=seed)
+    nbytes = int(wl.element_bytes().sum())
+    out = {"requests": count, "algorithmic_bytes": nbytes, "budget_bytes": 24 << 30, "slots": 4}
+
+    def served(arrival):
+        srv = serve.Server(dev, budget_bytes=24 << 30, slots=4, timing=True)
+        torch.cuda.synchronize()
+        srv.mark_start()
+        srv.submit_many(*wl.arrays(), arrival)
+        srv.run()
+        torch.cuda.synchronize()
+        lat = srv.done_gpu[:count] - srv.arrival[:count]
+        return srv, float(np.nanmax(srv.done_gpu[:count])), lat
+
+    def single(arrival):
+        reqs = [wl.request(i) for i in range(count)]
+        torch.cuda.synchronize()
+        start = torch.cuda.Event(enable_timing=True)
+        start.record()
+        t0 = time.perf_counter()
+        evs = []
+        for i, (op, x, aux) in enumerate(reqs):
+            if arrival is not None:
+                while time.perf_counter() - t0 < arrival[i]:
+                    pass
+            _, ev = serve.one_call_loop([(op, x, aux)])
+            evs.append(ev[0])
+        torch.cuda.synchronize()
+        done = np.array([start.elapsed_time(e) * 1e-3 for e in evs])
+        lat = done - (arrival if arrival is not None else 0.0)
+        return float(done.max()), lat
+
+    # warm-up: every class compiled / workspaces and pools allocated
+    warm = np.arange(min(count, 400))
+    srv = serve.Server(dev, budget_bytes=24 << 30, slots=4)
+    srv.submit_many(*wl.arrays(warm), np.zeros(warm.size))
+    srv.run()
+    serve.one_call_loop([wl.request(int(i)) for i in warm[:60]])
+    torch.cuda.synchronize()
+    del srv
+
+    srv, t_srv, _ = served(np.zeros(count))
+    t_one, _ = single(None)
+    out["served_req_per_s"] = count / t_srv
+    out["one_call_req_per_s"] = count / t_one
+    out["served_over_one_call"] = t_one / t_srv
+    out["served_GB/s"] = nbytes / t_srv / 1e9
+    out["batches"] = int(srv.batches)
+    out["peak_admitted_bytes"] = int(srv.peak_used)
+    del srv
+
+    lam = 0.5 * count / t_srv
+    rng = np.random.default_rng(seed + 1)
+    arrival = np.cumsum(rng.exponential(1.0 / lam, size=count))
+    srv, _, lat = served(arrival)
+    _, lat1 = single(arrival)
+    out["poisson_rate_req_per_s"] = lam
+    out["served_p50_ms"] = float(np.percentile(lat, 50) * 1e3)
+    out["served_p99_ms"] = float(np.percentile(lat, 99) * 1e3)
+    out["one_call_p50_ms"] = float(np.percentile(lat1, 50) * 1e3)
+    out["one_call_p99_ms"] = float(np.percentile(lat1, 99) * 1e3)
+    out["poisson_batches"] = int(srv.batches)
+    del srv
+
+    # accuracy sample: served in the mix vs single calls
+    idx = np.sort(np.random.default_rng(seed + 2).choice(count, size=min(sample, count), replace=False))
+    srv = serve.Server(dev, budget_bytes=24 << 30, slots=4, keep_results=True)
+    srv.submit_many(*wl.arrays(idx), np.zeros(idx.size))
+    srv.run()
+    exact_ok, max_rel = True, 0.0
+    for j, i in enumerate(idx):
+        op, x, aux = wl.request(int(i))
+        got = srv.result(j)
+        ref = serve.one_call_loop([(op, x, aux)])[0][0]
+        if x.dtype == torch.int8 or op == serve.COMPRESS:
+            exact_ok &= bool(torch.equal(got, ref))
+        else:
+            d = ((got.double() - ref.double()).abs() / ref.double().abs().clamp_min(1.0)).max().item()
+            max_rel = max(max_rel, d)
+    srv.release()
+    out["sample_checked"] = int(idx.size)
+    out["sample_integer_results_identical"] = exact_ok
+    out["sample_max_rel_diff_float"] = max_rel
+    del wl
+    torch.cuda.empty_cache()
+    return out
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -296,6 +400,57 @@ def run_reference_arm(args):
     return 0
 
 
+PROFILE_OPS = ("compress_f16", "compress_f32", "compress_ind_f16", "spmv_f32", "spmv_f16", "serve")
+
+
+def run_profile_op(args, dev):
+    """Diagnostics for profiler captures: one extra workload only (`--n`
+    elements for compaction, ~`--n` nonzeros on 2^20 rows for SpMV, `--requests`
+    requests of the served stream), `--warmup` untimed then `--steps` timed
+    runs; prints one JSON line with the device time per run."""
+    import numpy as np
+    import torch
+
+    import tcuscan_ops
+    from tcuscan_b200 import serve, workloads
+
+    op, n = args.profile_op, args.n
+    if op.startswith("compress"):
+        dt = torch.float32 if op == "compress_f32" else torch.float16
+        mask = workloads.bernoulli_mask(n, 0.3, dev, seed=8)
+        k = int(mask.sum().item())
+        xv = torch.randint(-1000, 1000, (n,), device=dev).to(dt)
+        eb = xv.element_size()
+        if op == "compress_ind_f16":
+            fn = lambda: tcuscan_ops.run_compress_ind_no_arange(xv, mask, 64)  # noqa: E731
+            nbytes = n * (eb + 1) + k * (eb + 4)
+        else:
+            fn = lambda: tcuscan_ops.run_compress_pos(xv, mask, k, 64)  # noqa: E731
+            nbytes = n * (eb + 1) + k * eb
+        units = n
+    elif op.startswith("spmv"):
+        dt = torch.float32 if op == "spmv_f32" else torch.float16
+        vals, indptr, cols, xs = workloads.zipf_csr(target_nnz=min(n, 1 << 26), dtype=dt, device=dev, seed=9)
+        fn = lambda: tcuscan_ops.run_spmv_v2(vals, indptr, cols, xs, 64)  # noqa: E731
+        eb = vals.element_size()
+        rows = indptr.numel() - 1
+        nbytes = vals.numel() * (eb + 4) + (rows + 1) * 4 + rows * 4 + xs.numel() * eb
+        units = vals.numel()
+    else:
+        wl = workloads.ServedStream(args.requests, dev, seed=11)
+        nbytes = int(wl.element_bytes().sum())
+        units = args.requests
+
+        def fn():
+            srv = serve.Server(dev, budget_bytes=24 << 30, slots=4)
+            srv.submit_many(*wl.arrays(), np.zeros(args.requests))
+            srv.run()
+    ms = _device_ms(fn, args.steps, args.warmup)
+    print(json.dumps({"profile_op": op, "units": units, "ms": ms, "GB/s": nbytes / (ms * 1e-3) / 1e9,
+                      "algorithmic_bytes": nbytes}), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -308,6 +463,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--phases", action="store_true", help="print a per-phase device-time breakdown (diagnostics)")
     ap.add_argument("--no-extras", action="store_true", help="headline workload only")
+    ap.add_argument("--profile-op", default=None, choices=PROFILE_OPS,
+                    help="diagnostics: run only this extra workload (for profiler captures)")
+    ap.add_argument("--requests", type=int, default=2000, help="served-stream requests for --profile-op serve")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -324,6 +482,8 @@ def main():
         import torch.distributed as dist
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+    if args.profile_op:
+        return run_profile_op(args, dev)
 
     import tcuscan_ops
 
@@ -425,6 +585,7 @@ def main():
     if rank == 0 and world == 1 and not args.no_extras:
         del x_host, z_host, x_dev
         extras = measure_extras(dev)
+        extras["served_stream"] = measure_serving(dev)
 
     cpu_base = None
     if rank == 0 and world == 1 and not args.no_cpu:

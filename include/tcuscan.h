@@ -154,9 +154,9 @@ TCU_API tcu_status_t tcu_scan_batch(const void* x, tcu_dtype_t x_dtype, int64_t 
                                     void* ws, size_t ws_bytes, void* stream);
 
 /* ---- stream compaction ---------------------------------------------------
- * Stable compaction of x[mask != 0] (elem_bytes = 1, 2, 4 or 8; int8 mask)
- * in one pass with a decoupled look-back; selected elements beyond
- * `capacity` are dropped.  idx_mode 0: values only; 1: also gather idx_in
+ * Stable compaction of x[mask != 0] (elem_bytes = 1, 2, 4 or 8; int8 mask):
+ * a count pass over the mask, a scan of the tile counts, then one streaming
+ * compaction pass; selected elements beyond `capacity` are dropped.  idx_mode 0: values only; 1: also gather idx_in
  * (idx_bytes = 4 or 8); 2: also write the selected positions (int32 when
  * idx_bytes = 4, int64 when 8).  count_dev (optional, 8-byte aligned device
  * int64) receives the number selected.
@@ -166,6 +166,28 @@ TCU_API tcu_status_t tcu_scan_batch(const void* x, tcu_dtype_t x_dtype, int64_t 
 TCU_API tcu_status_t tcu_compress(const void* x, int elem_bytes, const int8_t* mask, int64_t n, const void* idx_in,
                                   int idx_bytes, int idx_mode, void* out, void* idx_out, int64_t capacity,
                                   void* count_dev, void* ws, size_t ws_bytes, void* stream);
+/* The two halves of tcu_compress, for callers that size the output from
+ * the count first (run_compress reads the count back to the host, as the
+ * reference does, src/torch/torch_compress.h:62-64): tcu_compress_count
+ * counts the selected elements per tile, leaves the tile offsets in `ws` and
+ * writes the total (int64) to count_dev; tcu_compress_counted then compacts
+ * with those offsets.  The two calls take the same workspace, stream and
+ * element / index sizes, with no other use of the workspace between them. */
+TCU_API tcu_status_t tcu_compress_count(const int8_t* mask, int64_t n, int elem_bytes, int idx_mode, int idx_bytes,
+                                        void* count_dev, void* ws, size_t ws_bytes, void* stream);
+TCU_API tcu_status_t tcu_compress_counted(const void* x, int elem_bytes, const int8_t* mask, int64_t n,
+                                          const void* idx_in, int idx_bytes, int idx_mode, void* out, void* idx_out,
+                                          int64_t capacity, void* ws, size_t ws_bytes, void* stream);
+/* Compaction of several independent requests packed into one buffer (the
+ * serving loop batches compress calls this way): the stable compaction of
+ * x[mask != 0] over all n elements, plus seg_pos[i] = number of selected
+ * elements before seg_starts[i] (sorted int64 element offsets, one per
+ * request) and seg_pos[nseg] = the total.  Request i's result is
+ * out[seg_pos[i] : seg_pos[i+1]].  Batched form of run_compress
+ * (src/torch/torch_compress.h:41-98). */
+TCU_API tcu_status_t tcu_compress_segments(const void* x, int elem_bytes, const int8_t* mask, int64_t n,
+                                           const int64_t* seg_starts, int64_t nseg, void* out, int64_t capacity,
+                                           int64_t* seg_pos, void* ws, size_t ws_bytes, void* stream);
 /* Number of mask != 0 into a device uint64 (the reference sizes compress
  * outputs with run_reduce_tiles + .sum(), src/torch/torch_compress.h:62-64). */
 TCU_API tcu_status_t tcu_mask_count(const int8_t* mask, int64_t n, void* count_dev, void* stream);
@@ -198,6 +220,28 @@ TCU_API tcu_status_t tcu_complete_blocks(const void* x, tcu_dtype_t dtype, int64
 /* z = tril(ones(s, s)) in int8 / fp16 / bf16 / fp32 / int32.
  * Replaces run_gen_lower (src/torch/torch_gen_lower.h:31-59).            */
 TCU_API tcu_status_t tcu_gen_lower(int64_t s, tcu_dtype_t dtype, void* z, void* stream);
+
+/* ---- request packing (serving loop) ----------------------------------------
+ * The reference has no serving layer: each request is one run_* call
+ * (src/torch/torch_scan.h, torch_seg_ops.h, torch_compress.h).  The serving
+ * loop batches requests by packing them into one buffer and running one
+ * segmented launch; tcu_pack is the packing step.  `items` (device memory,
+ * sorted by dst, contiguous: items[0].dst == 0, items[i+1].dst == items[i].dst
+ * + items[i].len, total == sum of len) each copy n elements from src into
+ * dst[item.dst : item.dst + n] and zero the rest of the item's len.  src_bytes
+ * == dst_bytes copies elements of 1, 2, 4 or 8 bytes; src 4 -> dst 8 widens
+ * int32 to int64.  For 4- and 8-byte integer elements `add` is added to every
+ * copied element (rebasing row pointers by the request's offset); it must be
+ * zero for floating-point data.                                            */
+typedef struct tcu_pack_item {
+  const void* src;
+  int64_t dst;
+  int64_t n;
+  int64_t len;
+  int64_t add;
+} tcu_pack_item_t;
+TCU_API tcu_status_t tcu_pack(const tcu_pack_item_t* items, int64_t nitems, int src_bytes, int dst_bytes, void* dst,
+                              int64_t total, void* stream);
 
 #ifdef __cplusplus
 }

@@ -51,7 +51,7 @@ static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 }
 
 // 2-D row-major tensor [rows, cols] of `elem`-byte elements, box [box_rows,
-// box_cols], swizzle span = box_cols * elem bytes (32/64/128).
+// box_cols], swizzle span = box_cols * elem bytes (32/64/128; 16 = unswizzled).
 tcu_status_t make_map_2d(CUtensorMap* m, const void* base, CUtensorMapDataType dt, int elem, uint64_t cols,
                          uint64_t rows, uint32_t box_cols, uint32_t box_rows) {
   auto fn = encode_fn();
@@ -60,8 +60,10 @@ tcu_status_t make_map_2d(CUtensorMap* m, const void* base, CUtensorMapDataType d
     return TCU_ERR_DEVICE;
   }
   const uint32_t span = box_cols * elem;
-  CUtensorMapSwizzle sw = span == 128 ? CU_TENSOR_MAP_SWIZZLE_128B
-                                      : (span == 64 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B);
+  CUtensorMapSwizzle sw = span == 128  ? CU_TENSOR_MAP_SWIZZLE_128B
+                          : span == 64 ? CU_TENSOR_MAP_SWIZZLE_64B
+                          : span == 32 ? CU_TENSOR_MAP_SWIZZLE_32B
+                                       : CU_TENSOR_MAP_SWIZZLE_NONE;
   cuuint64_t dims[2] = {cols, rows};
   cuuint64_t strides[1] = {cols * (uint64_t)elem};
   cuuint32_t box[2] = {box_cols, box_rows};
@@ -254,9 +256,9 @@ void tcu_set_timeout_ns(uint64_t ns) { g_timeout_ns = ns ? ns : 4000000000ull; }
 uint64_t tcu_get_timeout_ns(void) { return g_timeout_ns; }
 
 size_t tcu_workspace_bytes(int64_t n, int S) {
-  (void)S;  // the smallest look-back tile of any kernel is 4096 elements
+  (void)S;  // the smallest look-back tile of any kernel is 2048 elements
   if (n < 0) n = 0;
-  const int64_t tiles = (n + 4095) / 4096 + 2;
+  const int64_t tiles = (n + 2047) / 2048 + 2;
   return 128 + (size_t)tiles * sizeof(TileDesc);
 }
 

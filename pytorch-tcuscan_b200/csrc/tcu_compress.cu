@@ -1,20 +1,37 @@
-// tcu_compress.cu -- single-pass stream compaction on B200.
+// tcu_compress.cu -- stream compaction on B200.
 //
 // Reference: run_compress / run_compress_pos / run_compress_ind /
 // run_compress_ind_no_arange (src/torch/torch_compress.h:41-309) count the
 // mask per block with reduce_tiles, read the total back to the host, then
 // gather with the vector GatherMask instruction (kernel_compress.h:97-208).
 //
-// Here compaction is byte/integer work bound by HBM, so it stays on the SIMT
-// cores: each CTA takes 256 x E elements per tile (tile ids from a global
-// counter), builds a 32-bit selection mask per thread from 16-byte mask
-// loads, publishes the tile's count at once, prefetches its x (and index)
-// values, looks back across tiles (int64 decoupled look-back) for its output
-// offset, compacts through shared memory and writes the compacted run with
-// coalesced stores.  The last tile writes the total count to device memory
-// so callers that cannot synchronise (CUDA graphs, the serving loop) never
-// need a host round trip.
+// Compaction is byte/integer work bound by HBM, so it stays on the SIMT cores
+// (no tensor-core reshaping).  Three launches, each a pure stream with no
+// waiting between CTAs:
+//   cmp_count_kernel    selected elements per tile (reads the mask once);
+//   cmp_offsets_kernel  one CTA: exclusive int64 scan of the tile counts ->
+//                       each tile's output offset, and the total;
+//   compress_kernel     one persistent CTA per SM, tiles assigned statically.
+//               warp 0 loads each tile's mask, values (and gathered indices)
+//               with 2-D TMA copies into a ring of shared-memory stages.  Each
+//               array is seen as rows of EPT elements, one row per worker
+//               thread, with the TMA swizzle of the row width, so every worker
+//               reads its own row without bank conflicts.
+//               warps 1-16: four worker warpgroups taking every fourth stage:
+//               selection bits from the mask row, the tile-local exclusive
+//               scan of the per-thread counts, compaction of the selected
+//               values from registers back into the stage (in place), then
+//               coalesced stores at the tile's precomputed offset.
+// run_compress needs the count on the host before it can size its output, so
+// the count pass is work it has to do anyway (tcu_compress_count, then
+// tcu_compress_counted); a single-pass look-back variant was measured slower
+// here: with 24-KB tiles every tile waited on its predecessors' counts.
+// The per-tile counts and offsets live in the workspace's descriptor region
+// and are zeroed after use (the region must hold only look-back descriptors
+// or zeros between launches).
 #include <cuda_runtime.h>
+
+#include <cstdio>
 
 #include "tcu_host.h"
 
@@ -23,19 +40,24 @@ namespace tcu {
 struct CompressParams {
   const void* x;
   const int8_t* mask;
-  const void* idx_in;   // optional gathered indices (compress_ind)
+  const void* idx_in;         // optional gathered indices (compress_ind)
   void* out;
-  void* idx_out;        // optional
+  void* idx_out;              // optional
   int64_t n;
-  int64_t capacity;     // elements the outputs can hold (compress_pos output_len)
+  int64_t capacity;           // elements the outputs can hold (compress_pos output_len)
   int64_t num_tiles;
-  long long* count_out; // optional: total selected (device)
+  int64_t full_rows;          // n / EPT: rows the tensor maps cover
+  int has_map;                // full_rows > 0
+  const long long* offsets;   // per-tile output offsets (workspace)
   WsHeader* ws;
-  TileDesc* descs;
   uint64_t timeout_ns;
 };
 
-constexpr int kCmpThreads = 256;
+constexpr int kCmpWG = 4;                       // worker warpgroups
+constexpr int kCmpThreads = 32 + 128 * kCmpWG;  // producer + workers
+constexpr int kCmpStageBudget = 200 * 1024;
+constexpr int kCmpMaxStages = 16;
+constexpr uint32_t kCmpSentinel = 0xFFFFFFFFu;
 
 template <int EB>
 struct ElemT;
@@ -47,6 +69,48 @@ template <>
 struct ElemT<4> { using T = uint32_t; };
 template <>
 struct ElemT<8> { using T = unsigned long long; };
+
+// Elements per worker row for an element / index size: at most 128 bytes of
+// payload per array and row; a tile is 128 rows.
+__host__ __device__ constexpr int cmp_ept(int eb, int ib) { return eb + ib <= 2 ? 64 : (eb + ib <= 4 ? 32 : 16); }
+
+template <int EB, int IDX, int IB>
+struct CmpCfg {
+  static constexpr int IBX = IDX ? IB : 0;     // index bytes held in the stage
+  static constexpr int RB = EB + IBX;
+  static constexpr int EPT = cmp_ept(EB, IBX);
+  static constexpr int TILE = 128 * EPT;
+  static constexpr int SPAN_M = EPT;           // bytes of one mask row
+  static constexpr int SPAN_X = EPT * EB;      // bytes of one value row
+  static constexpr int SPAN_I = EPT * (IB > 0 ? IB : 4);
+  static constexpr int X_OFF = TILE;
+  static constexpr int I_OFF = TILE * (1 + EB);
+  static constexpr int STAGE = TILE * (1 + RB);
+  static constexpr int NST_RAW = kCmpStageBudget / STAGE;
+  static constexpr int NST = NST_RAW > kCmpMaxStages ? kCmpMaxStages : NST_RAW;
+  static constexpr int CTRL = 1024;
+  static constexpr int SMEM = CTRL + NST * STAGE + 1024;  // + alignment slack
+  static_assert(NST >= kCmpWG + 1, "stage ring too short");
+  static_assert(SPAN_X <= 128 && SPAN_M <= 128 && (IDX == 0 || SPAN_I <= 128), "row span");
+  static_assert(STAGE % 1024 == 0, "stage alignment");
+};
+
+struct CmpCtrl {
+  uint64_t full[kCmpMaxStages];
+  uint64_t empty[kCmpMaxStages];
+  uint32_t stage_tid[kCmpMaxStages];
+  int wsum[kCmpWG][4];
+  int vote[kCmpWG][4];
+  int abort_flag;
+};
+static_assert(sizeof(CmpCtrl) <= 1024, "control block");
+
+// Byte address of 16-byte chunk v of row r in a TMA-swizzled area of
+// `span`-byte rows (span 16 = no swizzle).
+__device__ __forceinline__ uint32_t row_chunk(int r, int v, int span) {
+  const uint32_t o = (uint32_t)(r * span + 16 * v);
+  return span >= 32 ? swz(o, (uint32_t)span) : o;
+}
 
 // Element j of a run of 16-byte vectors held in registers (constant j after
 // unrolling, so the extraction is shifts and selects).
@@ -66,139 +130,317 @@ __device__ __forceinline__ typename ElemT<EB>::T vec_elem(const uint4* v, int j)
   }
 }
 
+// Sets element j of a register vector run (constant j after unrolling).
+template <int EB>
+__device__ __forceinline__ void vec_set(uint4* v, int j, typename ElemT<EB>::T e) {
+  constexpr int PER = 16 / EB;
+  uint4& w = v[j / PER];
+  const int b = (j % PER) * EB;
+  uint32_t lo;
+  if constexpr (EB >= 4) {
+    lo = (uint32_t)e;
+  } else {
+    constexpr uint32_t M = EB == 1 ? 0xFFu : 0xFFFFu;
+    const int sh = 8 * (b % 4);
+    const uint32_t cur = (b < 4) ? w.x : (b < 8) ? w.y : (b < 12) ? w.z : w.w;
+    lo = (cur & ~(M << sh)) | (((uint32_t)e & M) << sh);
+  }
+  if (b < 4) w.x = lo;
+  else if (b < 8) w.y = lo;
+  else if (b < 12) w.z = lo;
+  else w.w = lo;
+  if constexpr (EB == 8) {
+    const uint32_t hi = (uint32_t)((unsigned long long)e >> 32);
+    if (b < 4) w.y = hi;
+    else w.w = hi;
+  }
+}
+
 // IDX: 0 none, 1 gather idx_in (IB bytes), 2 positions (int32 when IB == 4,
 // int64 when IB == 8).
-template <int EB, int IDX, int IB, int E>
-__global__ void __launch_bounds__(kCmpThreads) compress_kernel(const CompressParams p) {
+template <int EB, int IDX, int IB>
+__global__ void __launch_bounds__(kCmpThreads, 1)
+    compress_kernel(const __grid_constant__ CUtensorMap mmap, const __grid_constant__ CUtensorMap xmap,
+                    const __grid_constant__ CUtensorMap imap, const CompressParams p) {
+  using C = CmpCfg<EB, IDX, IB>;
   using T = typename ElemT<EB>::T;
   using I = typename ElemT<(IB > 0 ? IB : 4)>::T;
-  constexpr int TILE = kCmpThreads * E;
-  extern __shared__ __align__(16) uint8_t s_dyn[];  // compacted values | indices
-  T* s_val = reinterpret_cast<T*>(s_dyn);
-  I* s_idx = reinterpret_cast<I*>(s_dyn + TILE * EB);
-  __shared__ uint32_t s_tid;
-  __shared__ int s_wsum[kCmpThreads / 32];
-  __shared__ long long s_prefix;
-  __shared__ uint32_t s_epoch;
-  __shared__ int s_abort;
+  constexpr int EPT = C::EPT;
+  constexpr int TILE = C::TILE;
+  constexpr int NST = C::NST;
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  CmpCtrl* ctl = reinterpret_cast<CmpCtrl*>(smem);
+  uint8_t* stages = smem + C::CTRL;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  WaitCtx wc{p.ws, &ctl->abort_flag, p.timeout_ns};
 
-  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-  WaitCtx wc{p.ws, &s_abort, p.timeout_ns};
-  if (t == 0) {
-    s_abort = 0;
-    s_epoch = *(volatile uint32_t*)&p.ws->epoch;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < NST; ++s) {
+      mbar_init(&ctl->full[s], 1);
+      mbar_init(&ctl->empty[s], 1);
+    }
+    ctl->abort_flag = 0;
+    fence_mbar_init();
+  }
+  if (warp == 0 && lane == 0 && p.has_map) {
+    prefetch_tmap(&mmap);
+    prefetch_tmap(&xmap);
+    if constexpr (IDX == 1) prefetch_tmap(&imap);
   }
   __syncthreads();
-  const uint32_t epoch = s_epoch;
 
-  while (true) {
-    if (t == 0) s_tid = atomicAdd(&p.ws->tile_counter, 1u);
-    __syncthreads();
-    const uint32_t tid = s_tid;
-    if ((int64_t)tid >= p.num_tiles || s_abort) break;
-    const int64_t e0 = (int64_t)tid * TILE + (int64_t)t * E;
-
-    // ---- mask -> selection bits ----
-    uint32_t sel = 0;
-    if (e0 + E <= p.n) {
-      const uint4* mv = reinterpret_cast<const uint4*>(p.mask + e0);
+  if (warp == 0) {
+    // ================= producer: this CTA's tiles, in order =================
+    if (lane == 0) {
+      uint32_t issued[kCmpMaxStages];
 #pragma unroll
-      for (int v = 0; v < E / 16; ++v) {
-        const uint4 w = __ldg(mv + v);
-        sel |= (sel4(w.x) | (sel4(w.y) << 4) | (sel4(w.z) << 8) | (sel4(w.w) << 12)) << (16 * v);
+      for (int s = 0; s < kCmpMaxStages; ++s) issued[s] = 0;
+      uint32_t seq = 0;
+      int sentinels = 0;  // one stop marker per worker warpgroup
+      int64_t tile = blockIdx.x;
+      while (sentinels < kCmpWG) {
+        const int s = seq % NST;
+        if (seq >= (uint32_t)NST && !mbar_wait(&ctl->empty[s], ((seq / NST) & 1u) ^ 1u, wc, 21, seq)) break;
+        const bool live = sentinels == 0 && tile < p.num_tiles && !aborted(wc);
+        const uint32_t tid = live ? (uint32_t)tile : kCmpSentinel;
+        ctl->stage_tid[s] = tid;
+        issued[s]++;
+        const int64_t row0 = tile * 128;
+        if (live && p.has_map && row0 < p.full_rows) {
+          uint8_t* st = stages + s * C::STAGE;
+          mbar_arrive_expect_tx(&ctl->full[s], (uint32_t)(TILE * (1 + EB + (IDX == 1 ? IB : 0))));
+          tma_load_2d(st, &mmap, 0, (int32_t)row0, &ctl->full[s]);
+          tma_load_2d(st + C::X_OFF, &xmap, 0, (int32_t)row0, &ctl->full[s]);
+          if constexpr (IDX == 1) tma_load_2d(st + C::I_OFF, &imap, 0, (int32_t)row0, &ctl->full[s]);
+        } else {
+          mbar_arrive(&ctl->full[s]);
+        }
+        if (live) tile += gridDim.x;
+        else ++sentinels;
+        ++seq;
       }
-    } else {
-      for (int j = 0; j < E; ++j)
-        if (e0 + j < p.n && p.mask[e0 + j] != 0) sel |= 1u << j;
+      // every copy issued must have landed before the CTA exits
+      for (int s = 0; s < NST; ++s)
+        if (issued[s]) mbar_drain(&ctl->full[s], (issued[s] - 1) & 1u, p.timeout_ns);
     }
-    const int cnt = __popc(sel);
+  } else {
+    // ================= worker warpgroups =================
+    const int w = (warp - 1) >> 2;
+    const int q = (warp - 1) & 3;
+    const int wg_thread = threadIdx.x - 32 - 128 * w;
+    const uint32_t bar_id = 1 + w;
+    for (uint32_t seq = w;; seq += kCmpWG) {
+      const int s = seq % NST;
+      int ok = 1;
+      if (lane == 0) ok = mbar_wait(&ctl->full[s], (seq / NST) & 1u, wc, 23, seq) ? 1 : 0;
+      ok = __shfl_sync(0xffffffffu, ok, 0);
+      if (lane == 0) ctl->vote[w][q] = ok;
+      named_bar_sync(bar_id, 128);
+      const int all_ok = ctl->vote[w][0] & ctl->vote[w][1] & ctl->vote[w][2] & ctl->vote[w][3];
+      const uint32_t tid = *(volatile uint32_t*)&ctl->stage_tid[s];
+      if (!all_ok || tid == kCmpSentinel) break;
+      const long long pre = p.offsets[tid];  // in flight while the stage is read
+      uint8_t* st = stages + s * C::STAGE;
+      const int64_t row = (int64_t)tid * 128 + wg_thread;
+      const int64_t e0 = row * EPT;  // first element of this thread's row
+      const bool in_smem = row < p.full_rows;
+      const bool is_tail = row == p.full_rows && e0 < p.n;
 
-    // ---- prefetch x / indices of selected elements ----
-    constexpr int XV = E * EB / 16;
-    constexpr int IV = (IDX == 1) ? E * IB / 16 : 1;
-    uint4 xv[XV];
-    uint4 iv[IV];
-    const bool full = e0 + E <= p.n;
-    if (sel && full) {
-      const uint4* xs = reinterpret_cast<const uint4*>(static_cast<const T*>(p.x) + e0);
+      // ---- selection bits and payload registers ----
+      unsigned long long sel = 0;
+      uint4 xr[C::SPAN_X / 16];
+      uint4 ir[IDX == 1 ? C::SPAN_I / 16 : 1];
+      if (in_smem) {
 #pragma unroll
-      for (int v = 0; v < XV; ++v) xv[v] = __ldg(xs + v);
-      if constexpr (IDX == 1) {
-        const uint4* is = reinterpret_cast<const uint4*>(static_cast<const I*>(p.idx_in) + e0);
+        for (int v = 0; v < C::SPAN_M / 16; ++v) {
+          const uint4 m = *reinterpret_cast<const uint4*>(st + row_chunk(wg_thread, v, C::SPAN_M));
+          sel |= (unsigned long long)(sel4(m.x) | (sel4(m.y) << 4) | (sel4(m.z) << 8) | (sel4(m.w) << 12)) << (16 * v);
+        }
+        if (sel) {
 #pragma unroll
-        for (int v = 0; v < IV; ++v) iv[v] = __ldg(is + v);
-      }
-    }
-    // ---- tile count: exclusive scan over threads ----
-    int inc = cnt;
+          for (int v = 0; v < C::SPAN_X / 16; ++v)
+            xr[v] = *reinterpret_cast<const uint4*>(st + C::X_OFF + row_chunk(wg_thread, v, C::SPAN_X));
+          if constexpr (IDX == 1) {
 #pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-      const int o = __shfl_up_sync(0xffffffffu, inc, d);
-      if (lane >= d) inc += o;
-    }
-    if (lane == 31) s_wsum[warp] = inc;
-    __syncthreads();
-    int wpre = 0, total = 0;
-#pragma unroll
-    for (int k = 0; k < kCmpThreads / 32; ++k) {
-      const int ws = s_wsum[k];
-      if (k < warp) wpre += ws;
-      total += ws;
-    }
-    const int local = wpre + inc - cnt;  // exclusive offset inside the tile
-
-    // ---- publish the count at once, then look back for the tile offset ----
-    if (warp == 0) {
-      if (lane == 0) publish_aggregate<long long>((int64_t)tid, (long long)total, 0, 0ll, p.descs, epoch);
-      const long long pre = warp_lookback<long long>((int64_t)tid, (long long)total, 0, 0ll, p.descs, epoch, wc, false);
-      if (lane == 0) {
-        s_prefix = pre;
-        if ((int64_t)tid == p.num_tiles - 1 && p.count_out) *p.count_out = pre + total;
-      }
-    }
-    // ---- compact into shared memory ----
-    {
-      int o = local;
-#pragma unroll
-      for (int j = 0; j < E; ++j) {
-        if (sel & (1u << j)) {
-          if (full) {
-            s_val[o] = vec_elem<EB>(xv, j);
-            if constexpr (IDX == 1) s_idx[o] = (I)vec_elem<(IB > 0 ? IB : 4)>(iv, j);
-          } else {  // ragged end of the input: scalar loads
-            s_val[o] = static_cast<const T*>(p.x)[e0 + j];
-            if constexpr (IDX == 1) s_idx[o] = static_cast<const I*>(p.idx_in)[e0 + j];
+            for (int v = 0; v < C::SPAN_I / 16; ++v)
+              ir[v] = *reinterpret_cast<const uint4*>(st + C::I_OFF + row_chunk(wg_thread, v, C::SPAN_I));
           }
-          if constexpr (IDX == 2) s_idx[o] = (I)(e0 + j);
-          ++o;
+        }
+      } else if (is_tail) {  // ragged end of the input: plain loads
+#pragma unroll
+        for (int v = 0; v < C::SPAN_X / 16; ++v) xr[v] = make_uint4(0, 0, 0, 0);
+#pragma unroll
+        for (int v = 0; v < (IDX == 1 ? C::SPAN_I / 16 : 1); ++v) ir[v] = make_uint4(0, 0, 0, 0);
+#pragma unroll
+        for (int j = 0; j < EPT; ++j) {
+          if (e0 + j < p.n && p.mask[e0 + j] != 0) {
+            sel |= 1ull << j;
+            vec_set<EB>(xr, j, static_cast<const T*>(p.x)[e0 + j]);
+            if constexpr (IDX == 1) vec_set<(IB > 0 ? IB : 4)>(ir, j, static_cast<const I*>(p.idx_in)[e0 + j]);
+          }
         }
       }
+      const int cnt = __popcll(sel);
+
+      // ---- tile-local exclusive scan of the per-thread counts ----
+      int inc = cnt;
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        const int o = __shfl_up_sync(0xffffffffu, inc, d);
+        if (lane >= d) inc += o;
+      }
+      if (lane == 31) ctl->wsum[w][q] = inc;
+      named_bar_sync(bar_id, 128);  // also: every row of the stage is in registers
+      int wpre = 0, total = 0;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int v = ctl->wsum[w][k];
+        if (k < q) wpre += v;
+        total += v;
+      }
+      const int local = wpre + inc - cnt;
+
+      // ---- compaction in place (values over the value rows, indices over the index rows) ----
+      {
+        T* sx = reinterpret_cast<T*>(st + C::X_OFF);
+        I* si = reinterpret_cast<I*>(st + C::I_OFF);
+        int o = local;
+#pragma unroll
+        for (int j = 0; j < EPT; ++j) {
+          if ((sel >> j) & 1ull) {
+            sx[o] = vec_elem<EB>(xr, j);
+            if constexpr (IDX == 1) si[o] = (I)vec_elem<(IB > 0 ? IB : 4)>(ir, j);
+            if constexpr (IDX == 2) si[o] = (I)(e0 + j);
+            ++o;
+          }
+        }
+      }
+      named_bar_sync(bar_id, 128);  // compacted run complete in shared memory
+
+      // ---- coalesced stores of the compacted run ----
+      {
+        const T* sx = reinterpret_cast<const T*>(st + C::X_OFF);
+        const I* si = reinterpret_cast<const I*>(st + C::I_OFF);
+        for (int i = wg_thread; i < total; i += 128) {
+          const long long g = pre + i;
+          if (g < p.capacity) {
+            static_cast<T*>(p.out)[g] = sx[i];
+            if constexpr (IDX != 0) static_cast<I*>(p.idx_out)[g] = si[i];
+          }
+        }
+      }
+      named_bar_sync(bar_id, 128);  // every thread is done with the stage
+      if (wg_thread == 0) mbar_arrive(&ctl->empty[s]);
+    }
+  }
+}
+
+// Selected elements of every tile (mask != 0).  One 256-thread CTA per tile
+// at a time, grid-stride over tiles.
+template <int TILE>
+__global__ void __launch_bounds__(256) cmp_count_kernel(const int8_t* __restrict__ mask, int64_t n, int64_t num_tiles,
+                                                        int* __restrict__ counts) {
+  constexpr int PER = TILE / 256;  // mask bytes per thread: 8, 16 or 32
+  __shared__ int s_w[8];
+  for (int64_t t = blockIdx.x; t < num_tiles; t += gridDim.x) {
+    const int64_t e = t * TILE + (int64_t)threadIdx.x * PER;
+    int c = 0;
+    if (e + PER <= n) {
+      if constexpr (PER >= 16) {
+        const uint4* mv = reinterpret_cast<const uint4*>(mask + e);
+#pragma unroll
+        for (int v = 0; v < PER / 16; ++v) {
+          const uint4 m = __ldg(mv + v);
+          c += __popc(sel4(m.x) | (sel4(m.y) << 4) | (sel4(m.z) << 8) | (sel4(m.w) << 12));
+        }
+      } else {
+        const uint2 m = __ldg(reinterpret_cast<const uint2*>(mask + e));
+        c += __popc(sel4(m.x) | (sel4(m.y) << 4));
+      }
+    } else {
+      for (int j = 0; j < PER; ++j)
+        if (e + j < n) c += mask[e + j] != 0;
+    }
+    c = warp_sum_any(c);
+    if ((threadIdx.x & 31) == 0) s_w[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int tot = 0;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) tot += s_w[k];
+      counts[t] = tot;
     }
     __syncthreads();
-    const long long pre = s_prefix;
-    // ---- coalesced write of the compacted run ----
-    for (int i = t; i < total; i += kCmpThreads) {
-      const long long gpos = pre + i;
-      if (gpos < p.capacity) {
-        static_cast<T*>(p.out)[gpos] = s_val[i];
-        if constexpr (IDX != 0) static_cast<I*>(p.idx_out)[gpos] = s_idx[i];
-      }
-    }
-    __syncthreads();  // shared buffers are reused by the next tile
   }
+}
 
-  // ---- teardown: the last CTA resets the counters and bumps the epoch ----
-  __syncthreads();
-  if (t == 0) {
-    __threadfence();
-    const uint32_t prev = atomicAdd(&p.ws->done_ctas, 1u);
-    if (prev == gridDim.x - 1) {
-      p.ws->tile_counter = 0;
-      p.ws->done_ctas = 0;
-      __threadfence();
-      atomicAdd(&p.ws->epoch, 1u);
-    }
+// Exclusive scan of the tile counts in one CTA: offsets[t] = selected before
+// tile t, offsets[num_tiles] = total, also written to *count_out.
+__global__ void __launch_bounds__(1024) cmp_offsets_kernel(const int* __restrict__ counts, int64_t num_tiles,
+                                                           long long* __restrict__ offsets, long long* count_out) {
+  __shared__ long long s_w[32];
+  const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
+  const int64_t per = (num_tiles + 1023) / 1024;
+  const int64_t b0 = (int64_t)t * per;
+  const int64_t b1 = b0 + per < num_tiles ? b0 + per : num_tiles;
+  long long sum = 0;
+  for (int64_t i = b0; i < b1; ++i) sum += counts[i];
+  long long inc = sum;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const long long o = __shfl_up_sync(0xffffffffu, inc, d);
+    if (lane >= d) inc += o;
   }
+  if (lane == 31) s_w[wid] = inc;
+  __syncthreads();
+  if (wid == 0) {
+    long long v = s_w[lane];
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const long long o = __shfl_up_sync(0xffffffffu, v, d);
+      if (lane >= d) v += o;
+    }
+    s_w[lane] = v;  // inclusive warp totals
+  }
+  __syncthreads();
+  long long run = (wid ? s_w[wid - 1] : 0) + inc - sum;
+  for (int64_t i = b0; i < b1; ++i) {
+    offsets[i] = run;
+    run += counts[i];
+  }
+  if (t == 1023) {
+    offsets[num_tiles] = s_w[31];
+    if (count_out) *count_out = s_w[31];
+  }
+}
+
+// Output position of every segment start: the number of selected elements
+// before it = the offset of its tile + the selected elements between the tile
+// start and the segment start.  One warp per segment start.
+__global__ void __launch_bounds__(256) seg_positions_kernel(const int8_t* __restrict__ mask, int64_t n,
+                                                            const long long* __restrict__ starts, int64_t nseg,
+                                                            const long long* __restrict__ offsets, int64_t tile,
+                                                            long long* __restrict__ pos) {
+  const int lane = threadIdx.x & 31;
+  const int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  if (i >= nseg) return;  // warp-uniform
+  long long s = starts[i];
+  s = s < 0 ? 0 : (s > n ? n : s);
+  const int64_t t = s / tile;
+  const long long base = offsets[t];
+  const int64_t e0 = t * tile;
+  const int64_t len = s - e0;
+  const int64_t nv = len / 16;
+  const uint4* mv = reinterpret_cast<const uint4*>(mask + e0);
+  unsigned long long c = 0;
+  for (int64_t v = lane; v < nv; v += 32) {
+    const uint4 w = __ldg(mv + v);
+    c += __popc(sel4(w.x) | (sel4(w.y) << 4) | (sel4(w.z) << 8) | (sel4(w.w) << 12));
+  }
+  for (int64_t e = nv * 16 + lane; e < len; e += 32) c += mask[e0 + e] != 0;
+  c = warp_sum_any(c);
+  if (lane == 0) pos[i] = base + (long long)c;
 }
 
 // Count of mask != 0 (the reference's reduce_tiles + .sum() used to size the
@@ -225,25 +467,134 @@ __global__ void __launch_bounds__(256) mask_count_kernel(const int8_t* mask, int
   }
 }
 
+// ---------------------------------------------------------------------------
+// Host side.  The tile is a function of the element and index sizes; the
+// per-tile counts and offsets sit in the workspace's descriptor region:
+// offsets[num_tiles + 1] (int64) then counts[num_tiles] (int32).
+static int64_t compress_tile(int elem_bytes, int idx_bytes) { return 128 * cmp_ept(elem_bytes, idx_bytes); }
+
+static int idx_stage_bytes(int idx_mode, int idx_bytes) { return idx_mode ? idx_bytes : 0; }
+
+struct CmpScratch {
+  long long* offsets;
+  int* counts;
+  int64_t tiles;
+  size_t bytes;
+};
+
+static tcu_status_t cmp_scratch(void* ws, size_t ws_bytes, int64_t n, int64_t tile, CmpScratch* sc) {
+  sc->tiles = (n + tile - 1) / tile;
+  sc->bytes = (size_t)(sc->tiles + 1) * 8 + (size_t)sc->tiles * 4;
+  if (!ws || ws_bytes < 128 + sc->bytes || ws_capacity(ws_bytes) < sc->tiles) return TCU_ERR_WORKSPACE;
+  sc->offsets = reinterpret_cast<long long*>(ws_descs(ws));
+  sc->counts = reinterpret_cast<int*>(sc->offsets + sc->tiles + 1);
+  return TCU_OK;
+}
+
+static tcu_status_t cmp_clear(void* ws, const CmpScratch& sc, cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(ws_descs(ws), 0, sc.bytes, st);
+  return e == cudaSuccess ? TCU_OK : cuda_fail(e, "cudaMemsetAsync(compress scratch)");
+}
+
+static tcu_status_t cmp_count(const int8_t* mask, int64_t n, int64_t tile, const CmpScratch& sc, long long* count_out,
+                              cudaStream_t st) {
+  int64_t grid = sc.tiles;
+  const int64_t cap = (int64_t)sm_count() * 8;
+  if (grid > cap) grid = cap;
+  if (tile == 8192) cmp_count_kernel<8192><<<(int)grid, 256, 0, st>>>(mask, n, sc.tiles, sc.counts);
+  else if (tile == 4096) cmp_count_kernel<4096><<<(int)grid, 256, 0, st>>>(mask, n, sc.tiles, sc.counts);
+  else cmp_count_kernel<2048><<<(int)grid, 256, 0, st>>>(mask, n, sc.tiles, sc.counts);
+  cmp_offsets_kernel<<<1, 1024, 0, st>>>(sc.counts, sc.tiles, sc.offsets, count_out);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? TCU_OK : cuda_fail(e, "compress count launch");
+}
+
 template <int EB, int IDX, int IB>
 static tcu_status_t launch_compress(CompressParams& p, cudaStream_t st) {
-  // elements per thread: keep the shared staging (256*E*(EB+IB) bytes) <= 32 KB
-  constexpr int E = (EB + IB) <= 4 ? 32 : 16;
-  constexpr int TILE = kCmpThreads * E;
-  p.num_tiles = (p.n + TILE - 1) / TILE;
-  const int smem = TILE * EB + (IDX ? TILE * IB : 0);
-  auto kern = compress_kernel<EB, IDX, IB, E>;
+  using C = CmpCfg<EB, IDX, IB>;
+  p.full_rows = p.n / C::EPT;
+  p.has_map = p.full_rows > 0 ? 1 : 0;
+  const int64_t rows = p.full_rows + (p.n % C::EPT ? 1 : 0);
+  p.num_tiles = (rows + 127) / 128;
+  if (p.num_tiles > 0x7FFFFFF0LL) return TCU_ERR_ARG;
+  CUtensorMap mm{}, xm{}, im{};
+  if (p.has_map) {
+    tcu_status_t s = make_map_2d(&mm, p.mask, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, C::SPAN_M, p.full_rows, C::SPAN_M, 128);
+    if (s == TCU_OK) s = make_map_2d(&xm, p.x, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, C::SPAN_X, p.full_rows, C::SPAN_X, 128);
+    if (s == TCU_OK && IDX == 1)
+      s = make_map_2d(&im, p.idx_in, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, C::SPAN_I, p.full_rows, C::SPAN_I, 128);
+    if (s != TCU_OK) return s;
+  }
+  auto kern = compress_kernel<EB, IDX, IB>;
   static bool attr_set = false;
   if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM);
     if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(compress)");
     attr_set = true;
   }
-  int grid = sm_count() * 3;
+  int grid = sm_count();
   if (p.num_tiles < grid) grid = (int)p.num_tiles;
-  kern<<<grid, kCmpThreads, smem, st>>>(p);
+  kern<<<grid, kCmpThreads, C::SMEM, st>>>(mm, xm, im, p);
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? TCU_OK : cuda_fail(e, "compress_kernel launch");
+}
+
+static tcu_status_t cmp_check(const void* x, int elem_bytes, const int8_t* mask, const void* idx_in, int idx_bytes,
+                              int idx_mode, const void* out, const void* idx_out) {
+  if (!x || !mask || !out) return TCU_ERR_ARG;
+  if (!aligned16(x) || !aligned16(mask) || !aligned16(out)) return TCU_ERR_ALIGN;
+  if (idx_mode < 0 || idx_mode > 2) return TCU_ERR_ARG;
+  if (idx_mode != 0 && (!idx_out || (idx_bytes != 4 && idx_bytes != 8))) return TCU_ERR_ARG;
+  if (idx_mode == 1 && (!idx_in || !aligned16(idx_in))) return idx_in ? TCU_ERR_ALIGN : TCU_ERR_ARG;
+  if (elem_bytes != 1 && elem_bytes != 2 && elem_bytes != 4 && elem_bytes != 8) return TCU_ERR_DTYPE;
+  return TCU_OK;
+}
+
+// The compaction pass, with the tile offsets already in the workspace.
+static tcu_status_t cmp_run(const void* x, int elem_bytes, const int8_t* mask, int64_t n, const void* idx_in,
+                            int idx_bytes, int idx_mode, void* out, void* idx_out, int64_t capacity,
+                            const CmpScratch& sc, void* ws, cudaStream_t st) {
+  CompressParams p{};
+  p.x = x;
+  p.mask = mask;
+  p.idx_in = idx_in;
+  p.out = out;
+  p.idx_out = idx_out;
+  p.n = n;
+  p.capacity = capacity;
+  p.offsets = sc.offsets;
+  p.ws = static_cast<WsHeader*>(ws);
+  p.timeout_ns = timeout_ns();
+#define TCU_CMP(EB, IDX, IB) return launch_compress<EB, IDX, IB>(p, st)
+  switch (elem_bytes) {
+    case 1:
+      if (idx_mode == 0) TCU_CMP(1, 0, 0);
+      if (idx_mode == 1) { if (idx_bytes == 4) TCU_CMP(1, 1, 4); TCU_CMP(1, 1, 8); }
+      if (idx_bytes == 4) TCU_CMP(1, 2, 4);
+      TCU_CMP(1, 2, 8);
+    case 2:
+      if (idx_mode == 0) TCU_CMP(2, 0, 0);
+      if (idx_mode == 1) { if (idx_bytes == 4) TCU_CMP(2, 1, 4); TCU_CMP(2, 1, 8); }
+      if (idx_bytes == 4) TCU_CMP(2, 2, 4);
+      TCU_CMP(2, 2, 8);
+    case 4:
+      if (idx_mode == 0) TCU_CMP(4, 0, 0);
+      if (idx_mode == 1) { if (idx_bytes == 4) TCU_CMP(4, 1, 4); TCU_CMP(4, 1, 8); }
+      if (idx_bytes == 4) TCU_CMP(4, 2, 4);
+      TCU_CMP(4, 2, 8);
+    default:
+      if (idx_mode == 0) TCU_CMP(8, 0, 0);
+      if (idx_mode == 1) { if (idx_bytes == 4) TCU_CMP(8, 1, 4); TCU_CMP(8, 1, 8); }
+      if (idx_bytes == 4) TCU_CMP(8, 2, 4);
+      TCU_CMP(8, 2, 8);
+  }
+#undef TCU_CMP
+}
+
+static tcu_status_t zero_count(void* count_dev, cudaStream_t st) {
+  if (!count_dev) return TCU_OK;
+  cudaError_t e = cudaMemsetAsync(count_dev, 0, sizeof(long long), st);
+  return e == cudaSuccess ? TCU_OK : cuda_fail(e, "cudaMemsetAsync(count)");
 }
 
 }  // namespace tcu
@@ -268,63 +619,84 @@ tcu_status_t tcu_mask_count(const int8_t* mask, int64_t n, void* count_dev, void
   return e == cudaSuccess ? TCU_OK : cuda_fail(e, "mask_count_kernel launch");
 }
 
+tcu_status_t tcu_compress_count(const int8_t* mask, int64_t n, int elem_bytes, int idx_mode, int idx_bytes,
+                                void* count_dev, void* ws, size_t ws_bytes, void* stream) {
+  if (n < 0) return TCU_ERR_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (n == 0) return zero_count(count_dev, st);
+  if (!mask) return TCU_ERR_ARG;
+  if (!aligned16(mask) || (reinterpret_cast<uintptr_t>(count_dev) & 7u)) return TCU_ERR_ALIGN;
+  if (elem_bytes != 1 && elem_bytes != 2 && elem_bytes != 4 && elem_bytes != 8) return TCU_ERR_DTYPE;
+  const int64_t tile = compress_tile(elem_bytes, idx_stage_bytes(idx_mode, idx_bytes));
+  CmpScratch sc;
+  tcu_status_t s = cmp_scratch(ws, ws_bytes, n, tile, &sc);
+  if (s != TCU_OK) return s;
+  return cmp_count(mask, n, tile, sc, static_cast<long long*>(count_dev), st);
+}
+
+tcu_status_t tcu_compress_counted(const void* x, int elem_bytes, const int8_t* mask, int64_t n, const void* idx_in,
+                                  int idx_bytes, int idx_mode, void* out, void* idx_out, int64_t capacity, void* ws,
+                                  size_t ws_bytes, void* stream) {
+  if (n < 0 || capacity < 0) return TCU_ERR_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (n == 0) return TCU_OK;
+  tcu_status_t s = cmp_check(x, elem_bytes, mask, idx_in, idx_bytes, idx_mode, out, idx_out);
+  if (s != TCU_OK) return s;
+  CmpScratch sc;
+  s = cmp_scratch(ws, ws_bytes, n, compress_tile(elem_bytes, idx_stage_bytes(idx_mode, idx_bytes)), &sc);
+  if (s != TCU_OK) return s;
+  s = cmp_run(x, elem_bytes, mask, n, idx_in, idx_bytes, idx_mode, out, idx_out, capacity, sc, ws, st);
+  if (s != TCU_OK) return s;
+  return cmp_clear(ws, sc, st);
+}
+
 tcu_status_t tcu_compress(const void* x, int elem_bytes, const int8_t* mask, int64_t n, const void* idx_in,
                           int idx_bytes, int idx_mode, void* out, void* idx_out, int64_t capacity, void* count_dev,
                           void* ws, size_t ws_bytes, void* stream) {
   if (n < 0 || capacity < 0) return TCU_ERR_ARG;
   cudaStream_t st = (cudaStream_t)stream;
+  if (n == 0) return zero_count(count_dev, st);
+  tcu_status_t s = cmp_check(x, elem_bytes, mask, idx_in, idx_bytes, idx_mode, out, idx_out);
+  if (s != TCU_OK) return s;
+  if (reinterpret_cast<uintptr_t>(count_dev) & 7u) return TCU_ERR_ALIGN;
+  const int64_t tile = compress_tile(elem_bytes, idx_stage_bytes(idx_mode, idx_bytes));
+  CmpScratch sc;
+  s = cmp_scratch(ws, ws_bytes, n, tile, &sc);
+  if (s == TCU_OK) s = cmp_count(mask, n, tile, sc, static_cast<long long*>(count_dev), st);
+  if (s == TCU_OK) s = cmp_run(x, elem_bytes, mask, n, idx_in, idx_bytes, idx_mode, out, idx_out, capacity, sc, ws, st);
+  if (s != TCU_OK) return s;
+  return cmp_clear(ws, sc, st);
+}
+
+tcu_status_t tcu_compress_segments(const void* x, int elem_bytes, const int8_t* mask, int64_t n,
+                                   const int64_t* seg_starts, int64_t nseg, void* out, int64_t capacity,
+                                   int64_t* seg_pos, void* ws, size_t ws_bytes, void* stream) {
+  if (n < 0 || nseg < 0 || capacity < 0 || !seg_pos || (nseg > 0 && !seg_starts)) return TCU_ERR_ARG;
+  if ((reinterpret_cast<uintptr_t>(seg_pos) & 7u) || (reinterpret_cast<uintptr_t>(seg_starts) & 7u))
+    return TCU_ERR_ALIGN;
+  cudaStream_t st = (cudaStream_t)stream;
   if (n == 0) {
-    if (count_dev) {
-      cudaError_t e = cudaMemsetAsync(count_dev, 0, sizeof(long long), st);
-      if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(count)");
-    }
-    return TCU_OK;
+    cudaError_t e = cudaMemsetAsync(seg_pos, 0, (size_t)(nseg + 1) * sizeof(int64_t), st);
+    return e == cudaSuccess ? TCU_OK : cuda_fail(e, "cudaMemsetAsync(seg_pos)");
   }
-  if (!x || !mask || !out) return TCU_ERR_ARG;
-  if (!aligned16(x) || !aligned16(mask) || !aligned16(out)) return TCU_ERR_ALIGN;
-  if (idx_mode < 0 || idx_mode > 2) return TCU_ERR_ARG;
-  if (idx_mode != 0 && (!idx_out || (idx_bytes != 4 && idx_bytes != 8))) return TCU_ERR_ARG;
-  if (idx_mode == 1 && (!idx_in || !aligned16(idx_in))) return idx_in ? TCU_ERR_ALIGN : TCU_ERR_ARG;
-  CompressParams p{};
-  p.x = x;
-  p.mask = mask;
-  p.idx_in = idx_in;
-  p.out = out;
-  p.idx_out = idx_out;
-  p.n = n;
-  p.capacity = capacity;
-  p.count_out = static_cast<long long*>(count_dev);
-  p.timeout_ns = timeout_ns();
-  const int64_t tiles_needed = (n + 4095) / 4096;
-  if (!ws || ws_capacity(ws_bytes) < tiles_needed) return TCU_ERR_WORKSPACE;
-  p.ws = static_cast<WsHeader*>(ws);
-  p.descs = ws_descs(ws);
-#define TCU_CMP(EB, IDX, IB) return launch_compress<EB, IDX, IB>(p, st)
-  switch (elem_bytes) {
-    case 1:
-      if (idx_mode == 0) TCU_CMP(1, 0, 0);
-      if (idx_mode == 1) { if (idx_bytes == 4) TCU_CMP(1, 1, 4); TCU_CMP(1, 1, 8); }
-      if (idx_bytes == 4) TCU_CMP(1, 2, 4);
-      TCU_CMP(1, 2, 8);
-    case 2:
-      if (idx_mode == 0) TCU_CMP(2, 0, 0);
-      if (idx_mode == 1) { if (idx_bytes == 4) TCU_CMP(2, 1, 4); TCU_CMP(2, 1, 8); }
-      if (idx_bytes == 4) TCU_CMP(2, 2, 4);
-      TCU_CMP(2, 2, 8);
-    case 4:
-      if (idx_mode == 0) TCU_CMP(4, 0, 0);
-      if (idx_mode == 1) { if (idx_bytes == 4) TCU_CMP(4, 1, 4); TCU_CMP(4, 1, 8); }
-      if (idx_bytes == 4) TCU_CMP(4, 2, 4);
-      TCU_CMP(4, 2, 8);
-    case 8:
-      if (idx_mode == 0) TCU_CMP(8, 0, 0);
-      if (idx_mode == 1) { if (idx_bytes == 4) TCU_CMP(8, 1, 4); TCU_CMP(8, 1, 8); }
-      if (idx_bytes == 4) TCU_CMP(8, 2, 4);
-      TCU_CMP(8, 2, 8);
-    default:
-      return TCU_ERR_DTYPE;
+  tcu_status_t s = cmp_check(x, elem_bytes, mask, nullptr, 0, 0, out, nullptr);
+  if (s != TCU_OK) return s;
+  const int64_t tile = compress_tile(elem_bytes, 0);
+  CmpScratch sc;
+  s = cmp_scratch(ws, ws_bytes, n, tile, &sc);
+  if (s == TCU_OK) s = cmp_count(mask, n, tile, sc, reinterpret_cast<long long*>(seg_pos + nseg), st);
+  if (s == TCU_OK) s = cmp_run(x, elem_bytes, mask, n, nullptr, 0, 0, out, nullptr, capacity, sc, ws, st);
+  if (s != TCU_OK) return s;
+  if (nseg > 0) {
+    const int64_t blocks = (nseg * 32 + 255) / 256;
+    if (blocks > 0x7FFFFFFF) return TCU_ERR_ARG;
+    seg_positions_kernel<<<(unsigned)blocks, 256, 0, st>>>(mask, n, reinterpret_cast<const long long*>(seg_starts),
+                                                           nseg, sc.offsets, tile,
+                                                           reinterpret_cast<long long*>(seg_pos));
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "seg_positions_kernel launch");
   }
-#undef TCU_CMP
+  return cmp_clear(ws, sc, st);
 }
 
 }  // extern "C"

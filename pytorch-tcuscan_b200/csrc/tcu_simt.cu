@@ -296,6 +296,15 @@ static tcu_status_t launched(const char* what) {
   return e == cudaSuccess ? TCU_OK : cuda_fail(e, what);
 }
 
+// Scratch written into a workspace's look-back descriptor region is zeroed
+// after use, so that the region only ever holds descriptors or zeros: stale
+// partial sums could otherwise read as a valid descriptor of a later launch
+// whose epoch happens to match their bits.
+static tcu_status_t clear_scratch(void* ws, size_t bytes, cudaStream_t st, const char* what) {
+  cudaError_t e = cudaMemsetAsync(static_cast<uint8_t*>(ws) + 128, 0, bytes, st);
+  return e == cudaSuccess ? launched(what) : cuda_fail(e, what);
+}
+
 }  // namespace tcu
 
 using namespace tcu;
@@ -366,7 +375,7 @@ tcu_status_t tcu_reduce_tiles(const void* x, tcu_dtype_t dtype, int64_t n, int64
   } else {
     return TCU_ERR_DTYPE;
   }
-  return launched("reduce_tiles");
+  return clear_scratch(ws, need - 128, st, "reduce_tiles");
 }
 
 tcu_status_t tcu_complete_rows(const void* x, tcu_dtype_t dtype, int64_t n, const void* sums, int num_blocks,
@@ -392,7 +401,7 @@ tcu_status_t tcu_complete_rows(const void* x, tcu_dtype_t dtype, int64_t n, cons
   } else {
     return TCU_ERR_DTYPE;
   }
-  return launched("complete_rows");
+  return clear_scratch(ws, need - 128, st, "complete_rows");
 }
 
 tcu_status_t tcu_complete_blocks(const void* x, tcu_dtype_t dtype, int64_t n, const void* sums, int num_blocks,

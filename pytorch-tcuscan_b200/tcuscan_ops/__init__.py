@@ -189,25 +189,39 @@ def _count(mask):
 
 
 def _compress(x, mask, out_len, idx_in=None, idx_mode=0, idx_dtype=torch.int32, where="run_compress"):
+    """Compaction into outputs of out_len elements (None: sized by a count
+    pass read back to the host, as the reference sizes its outputs)."""
     n = x.numel()
-    z = torch.empty(out_len, dtype=x.dtype, device=x.device)
-    idx_out = None
     ib = 0
     if idx_mode == 1:
-        idx_out = torch.empty(out_len, dtype=idx_in.dtype, device=x.device)
         ib = idx_in.element_size()
     elif idx_mode == 2:
+        ib = torch.empty((), dtype=idx_dtype).element_size()
+    sp = stream_ptr(x.device)
+    ws, wsb = workspace(x.device, _lib.lib.tcu_workspace_bytes(n, 64))
+    counted = out_len is None
+    if counted:
+        cnt = torch.empty(1, dtype=torch.int64, device=x.device)
+        check(_lib.lib.tcu_compress_count(mask.data_ptr(), n, x.element_size(), idx_mode, ib, cnt.data_ptr(), ws, wsb,
+                                          sp), where)
+        out_len = int(cnt.item())
+    z = torch.empty(out_len, dtype=x.dtype, device=x.device)
+    idx_out = None
+    if idx_mode == 1:
+        idx_out = torch.empty(out_len, dtype=idx_in.dtype, device=x.device)
+    elif idx_mode == 2:
         idx_out = torch.empty(out_len, dtype=idx_dtype, device=x.device)
-        ib = idx_out.element_size()
     if n == 0:
         return z, idx_out
-    ws, wsb = workspace(x.device, _lib.lib.tcu_workspace_bytes(n, 64))
-    st = _lib.lib.tcu_compress(
-        x.data_ptr(), x.element_size(), mask.data_ptr(), n,
-        idx_in.data_ptr() if idx_in is not None else None, ib, idx_mode,
-        z.data_ptr() if out_len > 0 else x.data_ptr(),
-        (idx_out.data_ptr() if out_len > 0 else x.data_ptr()) if idx_out is not None else None,
-        out_len, None, ws, wsb, stream_ptr(x.device))
+    zp = z.data_ptr() if out_len > 0 else x.data_ptr()
+    ip = (idx_out.data_ptr() if out_len > 0 else x.data_ptr()) if idx_out is not None else None
+    inp = idx_in.data_ptr() if idx_in is not None else None
+    if counted:
+        st = _lib.lib.tcu_compress_counted(x.data_ptr(), x.element_size(), mask.data_ptr(), n, inp, ib, idx_mode, zp,
+                                           ip, out_len, ws, wsb, sp)
+    else:
+        st = _lib.lib.tcu_compress(x.data_ptr(), x.element_size(), mask.data_ptr(), n, inp, ib, idx_mode, zp, ip,
+                                   out_len, None, ws, wsb, sp)
     check(st, where)
     _after(x)
     return z, idx_out
@@ -223,12 +237,11 @@ def run_compress(x, mask, S):
 
     The reference selects mask == 1 and sizes the output with sum(mask); both
     agree for 0/1 masks.  One count pass (read back to size the output, as
-    the reference does) and one single-pass compaction kernel."""
+    the reference does) and one streaming compaction pass."""
     _check_S_opt(S)
     x = _cuda_input(x)
     mask = _mask_input(mask, x.numel(), x.device)
-    k = int(_count(mask).item())
-    return _compress(x, mask, k)[0]
+    return _compress(x, mask, None)[0]
 
 
 def run_compress_pos(x, mask, output_len, S):
@@ -250,8 +263,7 @@ def run_compress_ind(x, indices_in, mask, S):
     if indices_in.element_size() not in (4, 8):
         raise TypeError("indices_in must be a 32- or 64-bit integer tensor")
     mask = _mask_input(mask, x.numel(), x.device)
-    k = int(_count(mask).item())
-    z, idx = _compress(x, mask, k, idx_in=indices_in, idx_mode=1, where="run_compress_ind")
+    z, idx = _compress(x, mask, None, idx_in=indices_in, idx_mode=1, where="run_compress_ind")
     return z, idx
 
 
@@ -261,8 +273,7 @@ def run_compress_ind_no_arange(x, mask, S):
     _check_S_opt(S)
     x = _cuda_input(x)
     mask = _mask_input(mask, x.numel(), x.device)
-    k = int(_count(mask).item())
-    return _compress(x, mask, k, idx_mode=2, where="run_compress_ind_no_arange")
+    return _compress(x, mask, None, idx_mode=2, where="run_compress_ind_no_arange")
 
 
 def run_filter_greater_eq(x, pivot, S):
