@@ -400,7 +400,8 @@ def run_reference_arm(args):
     return 0
 
 
-PROFILE_OPS = ("compress_f16", "compress_f32", "compress_ind_f16", "spmv_f32", "spmv_f16", "serve")
+PROFILE_OPS = ("compress_f16", "compress_f32", "compress_ind_f16", "spmv_f32", "spmv_f16", "serve", "segscan_i8",
+               "segscan_f16", "segsum_i8", "segsum_f16", "segsum_f32")
 
 
 def run_profile_op(args, dev):
@@ -436,6 +437,45 @@ def run_profile_op(args, dev):
         rows = indptr.numel() - 1
         nbytes = vals.numel() * (eb + 4) + (rows + 1) * 4 + rows * 4 + xs.numel() * eb
         units = vals.numel()
+    elif op.startswith("seg"):
+        # segmented scans over sorted bounds: "segscan" = few long segments
+        # (one per 2^20 elements, scan output), "segsum" = CSR-like segments of
+        # mean length 64 (per-segment sums)
+        dt = {"i8": torch.int8, "f16": torch.float16, "f32": torch.float32}[op.split("_")[1]]
+        xv = workloads.scan_input(n, dt, dev, seed=5)
+        eb = xv.element_size()
+        if op.startswith("segscan"):
+            bnd = torch.arange(0, n, 1 << 20, dtype=torch.int64, device=dev)
+            out = torch.empty(n, dtype=torch.int32 if dt == torch.int8 else torch.float32, device=dev)
+            nbytes = n * (eb + 4) + bnd.numel() * 8
+            sums = 0
+        else:
+            steps = torch.empty(n // 64 + 1024, device=dev).geometric_(1 / 64).to(torch.int64)
+            pts = torch.cumsum(steps, 0)
+            bnd = torch.cat([torch.zeros(1, dtype=torch.int64, device=dev), pts[pts < n],
+                             torch.full((1,), n, dtype=torch.int64, device=dev)])
+            out = torch.empty(bnd.numel() - 1, dtype=torch.int32 if dt == torch.int8 else torch.float32, device=dev)
+            nbytes = n * eb + bnd.numel() * 8 + out.numel() * 4
+            sums = 1
+        from tcuscan_ops import _lib as L
+
+        ws, wsb = L.workspace(dev, L.lib.tcu_workspace_bytes(n, 64))
+        sp = tcuscan_ops.stream_ptr(dev)
+
+        def fn():
+            tcuscan_ops.check(L.lib.tcu_seg_bounds(xv.data_ptr(), L.DTYPE_CODE[dt], n, 64, bnd.data_ptr(), L.TCU_INT64,
+                                                   bnd.numel(), sums, out.data_ptr(), ws, wsb, sp), op)
+        units = n
+        if args.phases:
+            fn()
+            torch.cuda.synchronize()
+            L.phase_times(dev, clear=True)
+            L.set_phase_profile(True)
+            for _ in range(5):
+                fn()
+            torch.cuda.synchronize()
+            L.set_phase_profile(False)
+            print(json.dumps({"phases_ns_sum_over_5_launches": L.phase_times(dev, clear=True)}), flush=True)
     else:
         wl = workloads.ServedStream(args.requests, dev, seed=11)
         nbytes = int(wl.element_bytes().sum())

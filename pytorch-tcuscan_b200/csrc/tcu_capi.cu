@@ -137,6 +137,20 @@ static tcu_status_t launch_scan_tc(const void* x, int64_t n, void* z, double sta
   p.out_sums = sa.out_sums;
   p.period = sa.period;
   p.seg_out = sa.seg_out;
+  // kSegBounds: every tile's first bound index, precomputed into the
+  // workspace after the tile descriptors (zeroed again after the scan, so the
+  // descriptor region never holds stale non-descriptor data)
+  long long* tile_first = nullptr;
+  if (MODE == kSegBounds && sa.nbounds > 0) {
+    if (ws_capacity(ws_bytes) < p.num_tiles + (p.num_tiles + 1) / 2 + 1) return TCU_ERR_WORKSPACE;
+    tile_first = reinterpret_cast<long long*>(p.descs + p.num_tiles);
+    int64_t grid = (sa.nbounds + 1 + 255) / 256;
+    const int64_t cap = (int64_t)sm_count() * 8;
+    if (grid > cap) grid = cap;
+    bounds_tiles_kernel<<<(int)grid, 256, 0, st>>>(sa.bounds, sa.bounds64, sa.nbounds, (int64_t)C::TILE_ELEMS,
+                                                    p.num_tiles, tile_first);
+    p.tile_first = tile_first;
+  }
 
   CUtensorMap in_map, out_map;
   std::memset(&in_map, 0, sizeof(in_map));
@@ -166,6 +180,10 @@ static tcu_status_t launch_scan_tc(const void* x, int64_t n, void* z, double sta
   kern<<<grid, kThreads, smem, st>>>(in_map, out_map, p);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "scan_tc_kernel launch");
+  if (tile_first) {
+    e = cudaMemsetAsync(tile_first, 0, (size_t)p.num_tiles * sizeof(long long), st);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(tile_first)");
+  }
   return TCU_OK;
 }
 

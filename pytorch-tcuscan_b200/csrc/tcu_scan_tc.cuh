@@ -65,6 +65,7 @@ struct ScanParams {
   int out_sums;          // kSegBounds: write one sum per segment instead of the scan
   int64_t period;        // kSegPeriodic
   void* seg_out;         // kSegBounds sums: nbounds - 1 entries (fp32 / int32)
+  const long long* tile_first;  // kSegBounds: first bound index of every tile (precomputed)
 };
 
 // Phase counters (nanoseconds summed over warpgroups / roles):
@@ -464,6 +465,86 @@ __device__ __forceinline__ long long warp_lower_bound(const ScanParams& p, long 
   return lo + __popc(__ballot_sync(0xffffffffu, below));
 }
 
+// tile_first[t] = first index i with bounds[i] >= t * tile_elems, for every
+// tile, in one pass over the (non-decreasing) bounds: bound k owns the tiles
+// after its predecessor's tile up to its own.  No search, O(nbounds + tiles).
+__global__ void __launch_bounds__(256) bounds_tiles_kernel(const void* bounds, int bounds64, int64_t nbounds,
+                                                           int64_t tile_elems, int64_t num_tiles,
+                                                           long long* __restrict__ tile_first) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k <= nbounds; k += stride) {
+    int64_t t_prev = -1, t_cur = num_tiles - 1;
+    if (k > 0) {
+      long long b = bounds64 ? __ldg(static_cast<const long long*>(bounds) + k - 1)
+                             : (long long)__ldg(static_cast<const int*>(bounds) + k - 1);
+      b = b < 0 ? 0 : b;
+      t_prev = b / tile_elems;
+    }
+    if (k < nbounds) {
+      long long b = bounds64 ? __ldg(static_cast<const long long*>(bounds) + k)
+                             : (long long)__ldg(static_cast<const int*>(bounds) + k);
+      b = b < 0 ? 0 : b;
+      const int64_t t = b / tile_elems;
+      t_cur = t < num_tiles - 1 ? t : num_tiles - 1;
+    }
+    for (int64_t t = t_prev + 1; t <= t_cur; ++t) tile_first[t] = k;
+  }
+}
+
+// Last segment start inside tile `tid` (elements [tid * tile, min(.., n))),
+// or -1: the largest bound in the tile for sorted bounds (the bounds of the
+// tile are [tile_first[tid], tile_first[tid + 1]); the last tile also skips
+// bounds at or past n), the largest multiple of the period for periodic
+// segments.  Warp-uniform result.
+template <int MODE>
+__device__ __forceinline__ long long tile_last_start(const ScanParams& p, uint32_t tid, int64_t tile) {
+  const int64_t e0 = (int64_t)tid * tile;
+  const int64_t e1 = e0 + tile < p.n ? e0 + tile : p.n;
+  if constexpr (MODE == kSegPeriodic) {
+    const int64_t m = ((e1 - 1) / p.period) * p.period;
+    return m >= e0 ? m : -1;
+  } else {
+    if (!p.tile_first || p.nbounds == 0) return -1;
+    const int lane = threadIdx.x & 31;
+    auto clampi = [&](long long v) { return v < 0 ? 0 : (v > p.nbounds ? p.nbounds : v); };
+    const long long i0 = clampi(__ldg(p.tile_first + tid));
+    const long long i1 = (int64_t)tid + 1 < p.num_tiles ? clampi(__ldg(p.tile_first + tid + 1)) : p.nbounds;
+    for (long long hi = i1 - 1; hi >= i0; hi -= 32) {
+      const long long kk = hi - lane;
+      const long long b = kk >= i0 ? bound_at(p, kk) : -1;
+      const unsigned ok = __ballot_sync(0xffffffffu, kk >= i0 && b >= e0 && b < e1);
+      if (ok) return __shfl_sync(0xffffffffu, b, __ffs(ok) - 1);
+      if (__shfl_sync(0xffffffffu, b, 31) >= 0 && __shfl_sync(0xffffffffu, b, 31) < e0) break;
+    }
+    return -1;
+  }
+}
+
+// Publishes the segmented aggregate of a tile from the summer's per-lane
+// sums: the ragged last row of the input is added from global memory (from
+// the last segment start on, when it lies in that row), then the warp total
+// goes out flagged as a segment start when the tile holds one.
+template <typename InT, int W, int MODE>
+__device__ __forceinline__ void ctl_publish_seg(const ScanParams& p, uint32_t tid, long long ls, int acci, float accf,
+                                                double accd, uint32_t epoch, int lane) {
+  using C = ScanCfg<InT, W, true>;
+  using V = typename std::conditional<C::IS_INT, long long, double>::type;
+  const int64_t e0 = (int64_t)tid * C::TILE_ELEMS;
+  const int64_t tail0 = p.full_rows * (int64_t)W;
+  if (p.tail > 0 && tail0 >= e0 && tail0 < e0 + C::TILE_ELEMS) {
+    const int64_t from = ls > tail0 ? ls : tail0;
+    for (int64_t e = from + lane; e < p.n; e += 32) {
+      if constexpr (C::IS_INT) acci += (int)static_cast<const int8_t*>(p.x)[e];
+      else if constexpr (C::IS_F32) accd += (double)static_cast<const float*>(p.x)[e];
+      else accf += load_elem<InT>(static_cast<const InT*>(p.x) + e);
+    }
+  }
+  V agg;
+  if constexpr (C::IS_INT) agg = (V)warp_sum_any(acci);
+  else agg = warp_sum_any((double)accf + accd);
+  if (lane == 0) publish_aggregate<V>((int64_t)tid, agg, ls >= 0 ? 1 : 0, V(0), p.descs, epoch);
+}
+
 // Summer warp: sums every tile straight from the TMA-filled SMEM stages (rows
 // past the input are skipped, the partial last row is read from global) and
 // publishes the tile aggregate at once, then hands (tile, aggregate) to the
@@ -481,6 +562,13 @@ __device__ __forceinline__ void scan_summer(const ScanParams& p, uint8_t* smem, 
   const int lane = threadIdx.x & 31;
   const V start = IS_INT ? (V)p.start_i : (V)p.start_f;
   const bool prof = p.phase_ns != nullptr && lane == 0;
+  // Modes whose tile aggregate this warp publishes as soon as the data lands:
+  // the full scan, and the segmented modes whose last segment start in a tile
+  // is known without reading the tile (sorted bounds, fixed period).  For the
+  // latter the aggregate is the sum after that start, flagged as a segment
+  // start, which ends every look-back that reaches the tile.
+  constexpr bool SEG_EARLY = (MODE == kSegBounds || MODE == kSegPeriodic);
+  constexpr bool SUMS = (MODE == kScanFull || SEG_EARLY);
   uint32_t k = 0;
   uint32_t i = 0;
   for (;; ++i) {
@@ -490,6 +578,7 @@ __device__ __forceinline__ void scan_summer(const ScanParams& p, uint8_t* smem, 
     float accf = 0.f;
     double accd = 0.0;
     int acci = 0;
+    long long ls = -1;  // last segment start of the tile (SEG_EARLY), -1 = none
     for (int j = 0; j < BPT; ++j, ++k) {
       const int s = k % C::NSTAGE;
       // every lane observes the TMA barrier before reading the stage
@@ -503,6 +592,28 @@ __device__ __forceinline__ void scan_summer(const ScanParams& p, uint8_t* smem, 
         break;
       }
       tid = cid;
+      if (SEG_EARLY && j == 0) ls = tile_last_start<MODE>(p, tid, C::TILE_ELEMS);
+      // rows of this block summed from shared memory: all valid rows, or
+      // (SEG_EARLY) those after the tile's last segment start; the start's
+      // own row is summed from its start column, from global memory
+      int r_lo = 0;
+      if (SEG_EARLY && ls >= 0) {
+        const int64_t be0 = (int64_t)tid * C::TILE_ELEMS + (int64_t)j * 128 * W;
+        if (ls >= be0 + 128 * (int64_t)W) {
+          r_lo = 128;
+        } else if (ls >= be0) {
+          const int lsr = (int)((ls - be0) / W);
+          r_lo = lsr + 1;
+          if (be0 / W + lsr < p.full_rows) {
+            const int64_t rend = be0 + (int64_t)(lsr + 1) * W;
+            for (int64_t e = ls + lane; e < rend; e += 32) {
+              if constexpr (IS_INT) acci += (int)static_cast<const int8_t*>(p.x)[e];
+              else if constexpr (C::IS_F32) accd += (double)static_cast<const float*>(p.x)[e];
+              else accf += load_elem<InT>(static_cast<const InT*>(p.x) + e);
+            }
+          }
+        }
+      }
       if constexpr (C::IS_F32) {
         // In-place split of the fp32 block: each 64-column row arrives as two
         // 128-byte halves (TMA boxes at +0 and +TERM_BYTES, same swizzle); the
@@ -522,7 +633,7 @@ __device__ __forceinline__ void scan_summer(const ScanParams& p, uint8_t* smem, 
           const float4 a = *reinterpret_cast<const float4*>(X0 + off);
           const float4 b = *reinterpret_cast<const float4*>(X1 + off);
           __syncwarp();
-          if (MODE == kScanFull && row < vrows)
+          if (SUMS && row < vrows && row >= r_lo)
             accd += (double)((a.x + a.y) + (a.z + a.w)) + (double)((b.x + b.y) + (b.z + b.w));
           uint2 ha, la, hb, lb;
           split_bf16x4(a, ha, la);
@@ -537,7 +648,7 @@ __device__ __forceinline__ void scan_summer(const ScanParams& p, uint8_t* smem, 
         __syncwarp();
         if (lane == 0) mbar_arrive(&ctl->conv[s]);
       }
-      if constexpr (MODE == kScanFull && !C::IS_F32) {
+      if constexpr (SUMS && !C::IS_F32) {
         const int64_t row0 = ((int64_t)tid * BPT + j) * 128;
         int64_t vr = p.full_rows - row0;
         const int vrows = vr <= 0 ? 0 : (vr >= 128 ? 128 : (int)vr);
@@ -545,7 +656,7 @@ __device__ __forceinline__ void scan_summer(const ScanParams& p, uint8_t* smem, 
 #pragma unroll
         for (int kb = 0; kb < C::KB; ++kb) {
           const uint4* src = (const uint4*)(smem + s * C::STAGE_BYTES + kb * (128 * C::SW));
-          for (int v = lane; v < nv; v += 32) {
+          for (int v = r_lo * (C::SW / 16) + lane; v < nv; v += 32) {
             const uint4 w = src[v];
             if constexpr (IS_INT) {
               acci = __dp4a((int)w.x, 0x01010101, acci);
@@ -568,8 +679,17 @@ __device__ __forceinline__ void scan_summer(const ScanParams& p, uint8_t* smem, 
     }
     if (stop) break;
     if constexpr (MODE == kSegBounds) {
-      // first bound index of the tile, found ahead of the epilogue
-      const long long i0 = warp_lower_bound(p, (long long)tid * C::TILE_ELEMS);
+      // first bound index of the tile (precomputed for every tile in one
+      // parallel pass over the bounds; clamped so a stale entry can never
+      // index outside them)
+      long long i0;
+      if (p.tile_first) {
+        i0 = __ldg(p.tile_first + tid);
+        i0 = i0 < 0 ? 0 : (i0 > p.nbounds ? p.nbounds : i0);
+      } else {
+        i0 = warp_lower_bound(p, (long long)tid * C::TILE_ELEMS);
+      }
+      ctl_publish_seg<InT, W, MODE>(p, tid, ls, acci, accf, accd, epoch, lane);
       int ok = 1;
       if (lane == 0) {
         const int m = i & 7;
@@ -580,6 +700,19 @@ __device__ __forceinline__ void scan_summer(const ScanParams& p, uint8_t* smem, 
         }
       }
       ok = __shfl_sync(0xffffffffu, ok, 0);
+      if (prof) phase_add(p, 5, globaltimer() - t0);
+      if (!ok) break;
+    }
+    if constexpr (MODE == kSegPeriodic) {
+      ctl_publish_seg<InT, W, MODE>(p, tid, ls, acci, accf, accd, epoch, lane);
+      int ok = 1;
+      if (lane == 0) {
+        const int m = i & 7;
+        if (i >= 8) ok = mbar_wait(&ctl->agg_empty[m], ((i >> 3) & 1u) ^ 1u, wc, 8, i) ? 1 : 0;
+        if (ok) mbar_arrive(&ctl->agg_full[m]);
+      }
+      ok = __shfl_sync(0xffffffffu, ok, 0);
+      if (prof) phase_add(p, 5, globaltimer() - t0);
       if (!ok) break;
     }
     if constexpr (MODE == kScanFull) {
@@ -725,6 +858,13 @@ __device__ __forceinline__ void seg_epilogue(const ScanParams& p, const CUtensor
       }
       if (wg_thread == 0) mbar_arrive(&ctl->agg_empty[m]);  // every thread has read tile_i0
     } else {
+      if constexpr (MODE == kSegPeriodic) {  // the summer has published this tile's aggregate
+        const int m = i & 7;
+        if (wg_thread == 0) {
+          mbar_wait(&ctl->agg_full[m], (i >> 3) & 1u, wc, 6, i);
+          mbar_arrive(&ctl->agg_empty[m]);
+        }
+      }
 #pragma unroll
       for (int j = 0; j < BPT; ++j) smask[j * 128 + r] = row_start_mask<W, MODE>(p, (row_tile0 + j * 128 + r) * W);
     }
@@ -741,30 +881,36 @@ __device__ __forceinline__ void seg_epilogue(const ScanParams& p, const CUtensor
         const bool is_tail = grow == p.full_rows && p.tail > 0;
         const bool live = grow < p.full_rows || is_tail;
         const unsigned long long mk = smask[j * 128 + r];
-        float accf = 0.f, basef = 0.f, prevf = 0.f;
-        int acci = 0, basei = 0, previ = 0;
-        bool seen = false;
-#pragma unroll
-        for (int c = 0; c < W / 16; ++c) {
-          uint32_t v[16];
-          tmem_ld16(tm + (uint32_t)(j * W + c * 16), v);
+        // row aggregate after the row's last segment start: z[W-1] - z[ls-1]
+        // (z[W-1] alone when the row holds no start).  Rows of a warp with
+        // no start and no ragged tail need only their last column.
+        uint32_t last, base = 0u;
+        if (!__any_sync(0xffffffffu, mk != 0ull || is_tail)) {
+          last = tmem_ld1(tm + (uint32_t)(j * W + W - 1));
           tmem_wait_ld();
-          if (is_tail) tail_chunk<InT, W>(p, c * 16, v, accf, acci);
+        } else {
+          uint32_t v[W];
 #pragma unroll
-          for (int e = 0; e < 16; ++e) {
-            const int col = c * 16 + e;
-            if ((mk >> col) & 1ull) {
-              basef = prevf;
-              basei = previ;
-              seen = true;
-            }
-            prevf = __uint_as_float(v[e]);
-            previ = (int)v[e];
+          for (int c = 0; c < W / 16; ++c)
+            tmem_ld16(tm + (uint32_t)(j * W + c * 16), *reinterpret_cast<uint32_t(*)[16]>(&v[c * 16]));
+          tmem_wait_ld();
+          if (is_tail) {
+            float accf = 0.f;
+            int acci = 0;
+#pragma unroll
+            for (int c = 0; c < W / 16; ++c)
+              tail_chunk<InT, W>(p, c * 16, *reinterpret_cast<uint32_t(*)[16]>(&v[c * 16]), accf, acci);
           }
+          if (mk != 0ull) {
+            const int ls = 63 - __clzll((long long)mk);
+#pragma unroll
+            for (int col = 0; col + 1 < W; ++col) base = (col == ls - 1) ? v[col] : base;
+          }
+          last = v[W - 1];
         }
-        // z[W-1] is prevf / previ; aggregate after the last start
-        if constexpr (IS_INT) tb[j] = live ? (uint32_t)(previ - (seen ? basei : 0)) : 0u;
-        else tb[j] = live ? __float_as_uint(prevf - (seen ? basef : 0.f)) : 0u;
+        const bool seen = mk != 0ull;
+        if constexpr (IS_INT) tb[j] = live ? (uint32_t)((int)last - (seen ? (int)base : 0)) : 0u;
+        else tb[j] = live ? __float_as_uint(__uint_as_float(last) - (seen ? __uint_as_float(base) : 0.f)) : 0u;
         fl[j] = (live && mk != 0ull) ? 1 : 0;
       }
       int rowf[BPT];
@@ -813,7 +959,10 @@ __device__ __forceinline__ void seg_epilogue(const ScanParams& p, const CUtensor
       if (prof) { const uint64_t t = globaltimer(); phase_add(p, 1, t - t_mark); t_mark = t; }
       // publish the (segmented) tile aggregate, then look back; a tile that
       // holds a segment start ends every look-back that reaches it
-      if (wg_thread == 0) publish_aggregate<V>((int64_t)tid, run, runf, V(0), p.descs, epoch);
+      // (sorted bounds and periodic segments: the summer warp published it
+      // as soon as the tile's data landed)
+      if (MODE != kSegBounds && MODE != kSegPeriodic && wg_thread == 0)
+        publish_aggregate<V>((int64_t)tid, run, runf, V(0), p.descs, epoch);
       const V pre = wg_lookback<V>((int64_t)tid, run, V(0), p.descs, epoch, wc, &ctl->lb[g], wg_thread, bar_id,
                                    runf);
 #pragma unroll

@@ -41,18 +41,37 @@ __device__ __forceinline__ int64_t pack_find(const tcu_pack_item_t* items, int64
   return lo;
 }
 
+// Same, searching forward from `from` (galloping: O(log distance) loads, one
+// or two when d lies in the same or the next item).
+__device__ __forceinline__ int64_t pack_gallop(const tcu_pack_item_t* items, int64_t nitems, int64_t from, int64_t d) {
+  int64_t lo = from, step = 1;
+  while (lo + step < nitems && items[lo + step].dst <= d) {
+    lo += step;
+    step <<= 1;
+  }
+  const int64_t hi = (lo + step < nitems ? lo + step : nitems) - 1;
+  return pack_find(items, lo, hi, d);
+}
+
+// Each CTA copies one contiguous range of the destination, chunk by chunk,
+// walking the (sorted) items forward; a chunk's first and last items are
+// found by thread 0 and each thread searches only between them.
 template <int SB, int DB>
 __global__ void __launch_bounds__(256) pack_kernel(const tcu_pack_item_t* __restrict__ items, int64_t nitems,
-                                                   uint8_t* __restrict__ dst, int64_t total) {
+                                                   uint8_t* __restrict__ dst, int64_t total, int64_t per_cta) {
   constexpr int VEC = 16 / DB;              // destination elements per 16-byte store
   constexpr int64_t CH = 256 * 4 * VEC;     // elements per chunk
   __shared__ int64_t s_range[2];
-  for (int64_t c = blockIdx.x; c * CH < total; c += gridDim.x) {
-    const int64_t c0 = c * CH;
-    const int64_t c1 = c0 + CH < total ? c0 + CH : total;
+  const int64_t r0 = (int64_t)blockIdx.x * per_cta;
+  const int64_t r1 = r0 + per_cta < total ? r0 + per_cta : total;
+  int64_t cursor = 0;  // thread 0: first item of the current chunk
+  if (threadIdx.x == 0 && r0 < r1) cursor = pack_find(items, 0, nitems - 1, r0);
+  for (int64_t c0 = r0; c0 < r1; c0 += CH) {
+    const int64_t c1 = c0 + CH < r1 ? c0 + CH : r1;
     if (threadIdx.x == 0) {
-      s_range[0] = pack_find(items, 0, nitems - 1, c0);
-      s_range[1] = pack_find(items, s_range[0], nitems - 1, c1 - 1);
+      cursor = pack_gallop(items, nitems, cursor, c0);
+      s_range[0] = cursor;
+      s_range[1] = pack_gallop(items, nitems, cursor, c1 - 1);
     }
     __syncthreads();
     const int64_t lo = s_range[0], hi = s_range[1];
@@ -96,10 +115,11 @@ template <int SB, int DB>
 static tcu_status_t launch_pack(const tcu_pack_item_t* items, int64_t nitems, void* dst, int64_t total,
                                 cudaStream_t st) {
   constexpr int64_t CH = 256 * 4 * (16 / DB);
-  int64_t chunks = (total + CH - 1) / CH;
+  const int64_t chunks = (total + CH - 1) / CH;
   const int64_t cap = (int64_t)sm_count() * 8;
-  const int grid = (int)(chunks < cap ? chunks : cap);
-  pack_kernel<SB, DB><<<grid, 256, 0, st>>>(items, nitems, static_cast<uint8_t*>(dst), total);
+  const int64_t grid = chunks < cap ? chunks : cap;
+  const int64_t per_cta = (chunks + grid - 1) / grid * CH;  // whole chunks: 16-byte aligned ranges
+  pack_kernel<SB, DB><<<(int)grid, 256, 0, st>>>(items, nitems, static_cast<uint8_t*>(dst), total, per_cta);
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? TCU_OK : cuda_fail(e, "pack_kernel launch");
 }
