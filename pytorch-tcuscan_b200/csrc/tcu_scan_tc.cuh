@@ -77,7 +77,7 @@ __device__ __forceinline__ void phase_add(const ScanParams& p, int k, uint64_t d
 }
 
 constexpr uint32_t kSentinel = 0xFFFFFFFFu;
-constexpr int kThreads = 352;  // 11 warps: producer, MMA, 2 epilogue warpgroups, summer
+constexpr int kThreads = 384;  // 12 warps: producer, MMA, 2 epilogue warpgroups, summer, second fp32 converter
 constexpr int kMaxSmem = 232448;
 
 template <typename InT, int W, bool SEG = false>
@@ -133,7 +133,8 @@ struct ScanCfg {
 struct ScanCtrl {
   uint64_t full[32];
   uint64_t empty[32];
-  uint64_t conv[32];                // fp32: stage converted to bf16 hi/lo operands
+  uint64_t conv[32];                // fp32: stage converted to bf16 hi/lo operands (two converter warps)
+  double cv_sum[32];                // fp32: sum of a stage's rows 64-127 (second converter)
   uint64_t tile_full[2];
   uint64_t slot_empty[2][16];
   uint64_t drain;
@@ -190,6 +191,38 @@ __device__ __forceinline__ void split_bf16x4(const float4 v, uint2& hi, uint2& l
   const __nv_bfloat162 l23 = __floats2bfloat162_rn(v.z - f23.x, v.w - f23.y);
   hi = make_uint2(*reinterpret_cast<const uint32_t*>(&h01), *reinterpret_cast<const uint32_t*>(&h23));
   lo = make_uint2(*reinterpret_cast<const uint32_t*>(&l01), *reinterpret_cast<const uint32_t*>(&l23));
+}
+
+// In-place split of rows [4 * it_lo, 4 * it_hi) of an fp32 block: each
+// 64-column row arrives as two 128-byte halves (TMA boxes at +0 and
+// +term_bytes, same swizzle); the row is rewritten as 64 bf16 hi = RN(x) in
+// the first slot and 64 bf16 lo = RN(x - hi) in the second, the two MMA
+// operand tiles.  A row is fully read (8 lanes x 2 x 16 B) before any lane
+// writes it.  Rows in [r_lo, vrows) are also summed into acc (FP32 per lane).
+__device__ __forceinline__ void convert_f32_rows(uint8_t* X0, int term_bytes, int it_lo, int it_hi, int r_lo,
+                                                 int vrows, bool sums, float& acc) {
+  uint8_t* X1 = X0 + term_bytes;
+  const int lane = threadIdx.x & 31;
+  const int rr = lane >> 3, cidx = lane & 7;
+#pragma unroll 4
+  for (int it = it_lo; it < it_hi; ++it) {
+    const int row = it * 4 + rr;
+    const uint32_t off = swz(row * 128 + cidx * 16, 128);
+    const float4 a = *reinterpret_cast<const float4*>(X0 + off);
+    const float4 b = *reinterpret_cast<const float4*>(X1 + off);
+    __syncwarp();
+    if (sums && row < vrows && row >= r_lo) acc += ((a.x + a.y) + (a.z + a.w)) + ((b.x + b.y) + (b.z + b.w));
+    uint2 ha, la, hb, lb;
+    split_bf16x4(a, ha, la);
+    split_bf16x4(b, hb, lb);
+    const int half = (cidx & 1) * 8;
+    *reinterpret_cast<uint2*>(X0 + swz(row * 128 + (cidx >> 1) * 16, 128) + half) = ha;
+    *reinterpret_cast<uint2*>(X0 + swz(row * 128 + (4 + (cidx >> 1)) * 16, 128) + half) = hb;
+    *reinterpret_cast<uint2*>(X1 + swz(row * 128 + (cidx >> 1) * 16, 128) + half) = la;
+    *reinterpret_cast<uint2*>(X1 + swz(row * 128 + (4 + (cidx >> 1)) * 16, 128) + half) = lb;
+  }
+  fence_proxy_async_smem();  // generic-proxy writes -> tcgen05 operand reads
+  __syncwarp();
 }
 
 template <typename InT>
@@ -615,38 +648,21 @@ __device__ __forceinline__ void scan_summer(const ScanParams& p, uint8_t* smem, 
         }
       }
       if constexpr (C::IS_F32) {
-        // In-place split of the fp32 block: each 64-column row arrives as two
-        // 128-byte halves (TMA boxes at +0 and +TERM_BYTES, same swizzle); the
-        // row is rewritten as 64 bf16 hi = RN(x) in the first slot and 64 bf16
-        // lo = RN(x - hi) in the second, the two MMA operand tiles.  A row is
-        // fully read (8 lanes x 2 x 16 B) before any lane writes it.
+        // rows 0-63 here, rows 64-127 by the second converter warp; the MMA
+        // waits for both (conv[s] counts two arrivals)
         uint8_t* X0 = smem + s * C::STAGE_BYTES;
-        uint8_t* X1 = X0 + C::TERM_BYTES;
-        const int rr = lane >> 3, cidx = lane & 7;
         const int64_t row0 = ((int64_t)tid * BPT + j) * 128;
         const int64_t vr = p.full_rows - row0;
         const int vrows = vr <= 0 ? 0 : (vr >= 128 ? 128 : (int)vr);
-#pragma unroll 4
-        for (int it = 0; it < 32; ++it) {
-          const int row = it * 4 + rr;
-          const uint32_t off = swz(row * 128 + cidx * 16, 128);
-          const float4 a = *reinterpret_cast<const float4*>(X0 + off);
-          const float4 b = *reinterpret_cast<const float4*>(X1 + off);
-          __syncwarp();
-          if (SUMS && row < vrows && row >= r_lo)
-            accd += (double)((a.x + a.y) + (a.z + a.w)) + (double)((b.x + b.y) + (b.z + b.w));
-          uint2 ha, la, hb, lb;
-          split_bf16x4(a, ha, la);
-          split_bf16x4(b, hb, lb);
-          const int half = (cidx & 1) * 8;
-          *reinterpret_cast<uint2*>(X0 + swz(row * 128 + (cidx >> 1) * 16, 128) + half) = ha;
-          *reinterpret_cast<uint2*>(X0 + swz(row * 128 + (4 + (cidx >> 1)) * 16, 128) + half) = hb;
-          *reinterpret_cast<uint2*>(X1 + swz(row * 128 + (cidx >> 1) * 16, 128) + half) = la;
-          *reinterpret_cast<uint2*>(X1 + swz(row * 128 + (4 + (cidx >> 1)) * 16, 128) + half) = lb;
-        }
-        fence_proxy_async_smem();  // generic-proxy writes -> tcgen05 operand reads
-        __syncwarp();
+        float acc = 0.f;
+        convert_f32_rows(X0, C::TERM_BYTES, 0, 16, r_lo, vrows, SUMS, acc);
+        accd += (double)acc;
         if (lane == 0) mbar_arrive(&ctl->conv[s]);
+        if constexpr (SUMS) {  // the other half's sum, stored before its conv arrival
+          const bool okc = __all_sync(0xffffffffu, mbar_wait(&ctl->conv[s], (k / C::NSTAGE) & 1u, wc, 9, i));
+          if (!okc) { stop = true; break; }
+          if (lane == 0) accd += ctl->cv_sum[s];
+        }
       }
       if constexpr (SUMS && !C::IS_F32) {
         const int64_t row0 = ((int64_t)tid * BPT + j) * 128;
@@ -739,6 +755,56 @@ __device__ __forceinline__ void scan_summer(const ScanParams& p, uint8_t* smem, 
       ok = __shfl_sync(0xffffffffu, ok, 0);
       if (prof) phase_add(p, 5, globaltimer() - t0);
       if (!ok) break;
+    }
+  }
+}
+
+// Second converter warp of fp32 launches: splits rows 64-127 of every stage
+// and leaves their sum (rows after the tile's last segment start, for the
+// modes whose aggregate the summer publishes) in cv_sum[s] before its conv
+// arrival.  Idle for the other input types.
+template <typename InT, int W, int MODE>
+__device__ __forceinline__ void scan_converter2(const ScanParams& p, uint8_t* smem, ScanCtrl* ctl,
+                                                const WaitCtx& wc) {
+  using C = ScanCfg<InT, W, is_seg(MODE)>;
+  if constexpr (C::IS_F32) {
+    constexpr int BPT = C::BPT;
+    constexpr bool SUMS = (MODE == kScanFull || MODE == kSegBounds || MODE == kSegPeriodic);
+    const int lane = threadIdx.x & 31;
+    uint32_t k = 0;
+    for (uint32_t i = 0;; ++i) {
+      long long ls = -1;
+      bool stop = false;
+      for (int j = 0; j < BPT; ++j, ++k) {
+        const int s = k % C::NSTAGE;
+        const bool ok = __all_sync(0xffffffffu, mbar_wait(&ctl->full[s], (k / C::NSTAGE) & 1u, wc, 10, i));
+        if (!ok) { stop = true; break; }
+        const uint32_t tid = *(volatile uint32_t*)&ctl->stage_cid[s];
+        if (tid == kSentinel) {
+          if (lane == 0) mbar_arrive(&ctl->conv[s]);
+          stop = true;
+          break;
+        }
+        if ((MODE == kSegBounds || MODE == kSegPeriodic) && j == 0) ls = tile_last_start<MODE>(p, tid, C::TILE_ELEMS);
+        int r_lo = 0;
+        if ((MODE == kSegBounds || MODE == kSegPeriodic) && ls >= 0) {
+          const int64_t be0 = (int64_t)tid * C::TILE_ELEMS + (int64_t)j * 128 * W;
+          if (ls >= be0 + 128 * (int64_t)W) r_lo = 128;
+          else if (ls >= be0) r_lo = (int)((ls - be0) / W) + 1;
+        }
+        const int64_t row0 = ((int64_t)tid * BPT + j) * 128;
+        const int64_t vr = p.full_rows - row0;
+        const int vrows = vr <= 0 ? 0 : (vr >= 128 ? 128 : (int)vr);
+        float acc = 0.f;
+        convert_f32_rows(smem + s * C::STAGE_BYTES, C::TERM_BYTES, 16, 32, r_lo, vrows, SUMS, acc);
+        if constexpr (SUMS) {
+          const double t = warp_sum_any((double)acc);
+          if (lane == 0) ctl->cv_sum[s] = t;
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&ctl->conv[s]);
+      }
+      if (stop) break;
     }
   }
 }
@@ -1091,7 +1157,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     for (int s = 0; s < C::NSTAGE; ++s) {
       mbar_init(&ctl->full[s], 1);
       mbar_init(&ctl->empty[s], 2);  // MMA commit + summer/converter arrive
-      mbar_init(&ctl->conv[s], 1);
+      mbar_init(&ctl->conv[s], 2);
     }
     for (int m = 0; m < 8; ++m) {
       mbar_init(&ctl->agg_full[m], 1);
@@ -1240,8 +1306,10 @@ __global__ void __launch_bounds__(kThreads, 1)
   } else if (warp < 10) {
     if constexpr (is_seg(MODE)) seg_epilogue<InT, W, MODE>(p, out_map, smem, ctl, tmem_base, epoch, wc);
     else scan_epilogue<InT, W, MODE>(p, out_map, smem, ctl, tmem_base, epoch, wc);
-  } else {
+  } else if (warp == 10) {
     scan_summer<InT, W, MODE>(p, smem, ctl, epoch, wc);
+  } else {
+    scan_converter2<InT, W, MODE>(p, smem, ctl, wc);
   }
 
   // ---- teardown ----
