@@ -911,16 +911,22 @@ __device__ __forceinline__ void seg_epilogue(const ScanParams& p, const CUtensor
       for (int j = 0; j < BPT; ++j) smask[j * 128 + r] = 0ull;
       named_bar_sync(bar_id, 128);
       cur = *(volatile long long*)&ctl->tile_i0[m];
-      for (long long base = cur;; base += 128) {
-        const long long idx = base + wg_thread;
-        const long long b = idx < p.nbounds ? bound_at(p, idx) : LLONG_MAX;
-        const bool in = b < tile_e1;
-        if (in && b >= tile_e0) {
-          const long long off = b - tile_e0;
-          const int row = (int)(off / W);
-          atomicOr(&smask[row], 1ull << (off % W));
+      // 512 bounds per round: four independent loads per thread in flight
+      for (long long base = cur;; base += 512) {
+        long long bb[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const long long idx = base + wg_thread + 128 * u;
+          bb[u] = idx < p.nbounds ? bound_at(p, idx) : LLONG_MAX;
         }
-        if (wg_count(in, votes, lane, q, bar_id) < 128) break;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          if (bb[u] < tile_e1 && bb[u] >= tile_e0) {
+            const long long off = bb[u] - tile_e0;
+            atomicOr(&smask[(int)(off / W)], 1ull << (off % W));
+          }
+        }
+        if (wg_count(bb[3] < tile_e1, votes, lane, q, bar_id) < 128) break;
       }
       if (wg_thread == 0) mbar_arrive(&ctl->agg_empty[m]);  // every thread has read tile_i0
     } else {
@@ -967,10 +973,31 @@ __device__ __forceinline__ void seg_epilogue(const ScanParams& p, const CUtensor
             for (int c = 0; c < W / 16; ++c)
               tail_chunk<InT, W>(p, c * 16, *reinterpret_cast<uint32_t(*)[16]>(&v[c * 16]), accf, acci);
           }
-          if (mk != 0ull) {
-            const int ls = 63 - __clzll((long long)mk);
+          if (mk != 0ull && sums_out) {
+            // per-segment sums issue no TMA stores, so the staging buffer is
+            // free here: the row goes through it and z[ls - 1] is read back
+            const int t = 62 - __clzll((long long)mk);  // ls - 1 (-1: start at column 0)
 #pragma unroll
-            for (int col = 0; col + 1 < W; ++col) base = (col == ls - 1) ? v[col] : base;
+            for (int e4 = 0; e4 < W / 4; ++e4) {
+              const int box = (e4 * 4) / C::OBW, cin = (e4 * 4) % C::OBW;
+              *(uint4*)(stg_base + box * (128 * C::OSW) + swz(r * C::OSW + cin * 4, C::OSW)) =
+                  make_uint4(v[e4 * 4], v[e4 * 4 + 1], v[e4 * 4 + 2], v[e4 * 4 + 3]);
+            }
+            base = t < 0 ? 0u : stage_lookup(stg_base, (int64_t)r * W + t, W, C::OBW, C::OSW);
+          } else if (mk != 0ull) {
+            // base = z[ls - 1], the value before the row's last start ls
+            // (four independent select chains, then one pick)
+            const int t = 62 - __clzll((long long)mk);  // ls - 1 (-1: start at column 0)
+            uint32_t part[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+            for (int q4 = 0; q4 < 4; ++q4)
+#pragma unroll
+              for (int c = 0; c < W / 4; ++c) {
+                const int col = q4 * (W / 4) + c;
+                part[q4] = (col == t) ? v[col] : part[q4];
+              }
+            const int qsel = t < 0 ? 0 : t / (W / 4);
+            base = t < 0 ? 0u : (qsel == 0 ? part[0] : qsel == 1 ? part[1] : qsel == 2 ? part[2] : part[3]);
           }
           last = v[W - 1];
         }
@@ -1044,12 +1071,19 @@ __device__ __forceinline__ void seg_epilogue(const ScanParams& p, const CUtensor
       const int64_t grow = brow0 + r;
       const bool is_tail = (grow == p.full_rows) && p.tail > 0;
       const unsigned long long mk = smask[j * 128 + r];
-      float accf = 0.f, basef = 0.f, prevf = 0.f;
-      int acci = 0, basei = 0, previ = 0;
-      bool seen = false;
+      float accf = 0.f;
+      int acci = 0;
       const float cf = IS_INT ? 0.f : (float)rowex[j];
       const uint32_t ci = IS_INT ? (uint32_t)(long long)rowex[j] : 0u;
       uint8_t* stg = stg_base + (nfill % C::STG_BUFS) * C::STG_BYTES;
+      // per-segment sums: the first chunk of this block's bounds is loaded
+      // now, its latency hidden behind the row work below
+      long long pf_b = LLONG_MAX, pf_bp = 0;
+      if (sums_out) {
+        const long long idx = cur + wg_thread;
+        if (idx < p.nbounds) pf_b = bound_at(p, idx);
+        if (idx >= 1 && idx - 1 < p.nbounds) pf_bp = bound_at(p, idx - 1);
+      }
       if (wg_thread == 0) {
         if (C::STG_BUFS == 2) bulk_wait_read1(); else bulk_wait_read0();
       }
@@ -1067,31 +1101,50 @@ __device__ __forceinline__ void seg_epilogue(const ScanParams& p, const CUtensor
         for (int c = 0; c < W / 16; ++c)
           tail_chunk<InT, W>(p, c * 16, *reinterpret_cast<uint32_t(*)[16]>(&v[c * 16]), accf, acci);
       }
+      if (sums_out) {
+        // per-segment sums need y only at segment ends: stage the raw row
+        // prefixes z and keep the row's carry (in place of its start mask,
+        // which this path no longer reads); the sums loop below forms
+        // y[e] = z[e] - z[s - 1] or z[e] + carry with the same arithmetic
 #pragma unroll
-      for (int e4 = 0; e4 < W / 4; ++e4) {
-        uint32_t o[4];
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          const int col = e4 * 4 + e;
-          if ((mk >> col) & 1ull) {
-            basef = prevf;
-            basei = previ;
-            seen = true;
-          }
-          const uint32_t z = v[col];
-          if constexpr (IS_INT) o[e] = seen ? (uint32_t)((int)z - basei) : z + ci;
-          else o[e] = __float_as_uint(seen ? __uint_as_float(z) - basef : __uint_as_float(z) + cf);
-          prevf = __uint_as_float(z);
-          previ = (int)z;
+        for (int e4 = 0; e4 < W / 4; ++e4) {
+          const int box = (e4 * 4) / C::OBW, cin = (e4 * 4) % C::OBW;
+          *(uint4*)(stg + box * (128 * C::OSW) + swz(r * C::OSW + cin * 4, C::OSW)) =
+              make_uint4(v[e4 * 4], v[e4 * 4 + 1], v[e4 * 4 + 2], v[e4 * 4 + 3]);
         }
-        const int cc = e4 * 4;
-        const int box = cc / C::OBW, cin = cc % C::OBW;
-        *(uint4*)(stg + box * (128 * C::OSW) + swz(r * C::OSW + cin * 4, C::OSW)) = make_uint4(o[0], o[1], o[2], o[3]);
-        if (is_tail && !sums_out) {
-          uint32_t* zt = (uint32_t*)p.z + p.full_rows * (int64_t)W + cc;
+        smask[j * 128 + r] = IS_INT ? (unsigned long long)ci : (unsigned long long)__float_as_uint(cf);
+      }
+      // y[col] = z[col] - sub, with sub = -carry before the row's first
+      // segment start and z[s - 1] (0 for s = 0) from a start s on; z + c and
+      // z - (-c) round identically, so this matches the carry-add form
+      const uint32_t mlo = (uint32_t)mk, mhi = (uint32_t)(mk >> 32);
+      uint32_t subi = 0u - ci;
+      float subf = -cf;
+      if (!sums_out) {
 #pragma unroll
-          for (int e = 0; e < 4; ++e)
-            if (cc + e < p.tail) zt[e] = o[e];
+        for (int e4 = 0; e4 < W / 4; ++e4) {
+          uint32_t o[4];
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            const int col = e4 * 4 + e;
+            const bool st = ((col < 32 ? mlo : mhi) >> (col & 31)) & 1u;
+            if (st) {
+              subi = col ? v[col - 1] : 0u;
+              subf = col ? __uint_as_float(v[col - 1]) : 0.f;
+            }
+            if constexpr (IS_INT) o[e] = v[col] - subi;
+            else o[e] = __float_as_uint(__uint_as_float(v[col]) - subf);
+          }
+          const int cc = e4 * 4;
+          const int box = cc / C::OBW, cin = cc % C::OBW;
+          *(uint4*)(stg + box * (128 * C::OSW) + swz(r * C::OSW + cin * 4, C::OSW)) =
+              make_uint4(o[0], o[1], o[2], o[3]);
+          if (is_tail) {
+            uint32_t* zt = (uint32_t*)p.z + p.full_rows * (int64_t)W + cc;
+#pragma unroll
+            for (int e = 0; e < 4; ++e)
+              if (cc + e < p.tail) zt[e] = o[e];
+          }
         }
       }
       fence_proxy_async_smem();
@@ -1112,12 +1165,25 @@ __device__ __forceinline__ void seg_epilogue(const ScanParams& p, const CUtensor
         const int64_t be1 = min(be0 + 128 * (int64_t)W, p.n);
         for (long long base = cur;; base += 128) {
           const long long idx = base + wg_thread;
-          const long long b = idx < p.nbounds ? bound_at(p, idx) : LLONG_MAX;
+          const bool first = base == cur;
+          const long long b = first ? pf_b : (idx < p.nbounds ? bound_at(p, idx) : LLONG_MAX);
           const bool in = b <= be1;
           if (in && idx >= 1 && (b > be0 || (be0 == 0 && b == 0))) {
-            const long long bp = bound_at(p, idx - 1);
+            const long long bp = first ? pf_bp : bound_at(p, idx - 1);
             uint32_t val = 0u;
-            if (b > bp && b > be0) val = stage_lookup(stg, b - 1 - be0, W, C::OBW, C::OSW);
+            if (b > bp && b > be0) {
+              const int64_t e = b - 1 - be0;  // the segment's last element, local
+              const int er = (int)(e / W);
+              const int64_t rs = be0 + (int64_t)er * W;
+              const uint32_t ze = stage_lookup(stg, e, W, C::OBW, C::OSW);
+              if (bp >= rs) {  // the segment starts in this row
+                const uint32_t zs = bp > rs ? stage_lookup(stg, bp - 1 - be0, W, C::OBW, C::OSW) : 0u;
+                val = IS_INT ? ze - zs : __float_as_uint(__uint_as_float(ze) - __uint_as_float(zs));
+              } else {  // it entered the row from above: add the row's carry
+                const uint32_t c = (uint32_t)smask[j * 128 + er];
+                val = IS_INT ? ze + c : __float_as_uint(__uint_as_float(ze) + __uint_as_float(c));
+              }
+            }
             static_cast<uint32_t*>(p.seg_out)[idx - 1] = val;
           }
           const int nin = wg_count(in, votes, lane, q, bar_id);
