@@ -72,9 +72,10 @@ TCU_API tcu_status_t tcu_workspace_init(void* ws, size_t ws_bytes, void* stream)
 TCU_API tcu_status_t tcu_workspace_error(void* ws, uint32_t info[3], int clear, void* stream);
 /* Diagnostics: when enabled, the scan kernels add per-phase device time (ns)
  * to eight counters in the workspace: 0 epilogue wait for the MMA, 1 row
- * totals, 2 look-back, 3 drain, 4 producer stage waits, 5 MMA data waits,
- * 6 MMA TMEM waits, 7 tiles.  Read (and optionally clear) them with
- * tcu_workspace_phase_ns (synchronises the stream).  Off by default. */
+ * totals, 2 look-back, 3 drain, 4 producer stage waits, 5 summer warp (its
+ * waits included), 6 summer waits for landed data, 7 tiles.  Read (and
+ * optionally clear) them with tcu_workspace_phase_ns (synchronises the
+ * stream).  Off by default. */
 TCU_API void tcu_set_phase_profile(int enable);
 TCU_API tcu_status_t tcu_workspace_phase_ns(void* ws, uint64_t out[8], int clear, void* stream);
 

@@ -71,7 +71,7 @@ struct ScanParams {
 // Phase counters (nanoseconds summed over warpgroups / roles):
 // 0 epilogue wait for the MMA, 1 row totals, 2 look-back, 3 drain,
 // 4 producer waits for free stages, 5 summer (including its waits for data),
-// 6 unused, 7 tiles processed.
+// 6 summer waits for landed data (part of 5), 7 tiles processed.
 __device__ __forceinline__ void phase_add(const ScanParams& p, int k, uint64_t dt) {
   if (p.phase_ns) atomicAdd(p.phase_ns + k, (unsigned long long)dt);
 }
@@ -615,7 +615,9 @@ __device__ __forceinline__ void scan_summer(const ScanParams& p, uint8_t* smem, 
     for (int j = 0; j < BPT; ++j, ++k) {
       const int s = k % C::NSTAGE;
       // every lane observes the TMA barrier before reading the stage
+      const uint64_t tw = prof ? globaltimer() : 0;
       const bool ok = __all_sync(0xffffffffu, mbar_wait(&ctl->full[s], (k / C::NSTAGE) & 1u, wc, 7, i));
+      if (prof) phase_add(p, 6, globaltimer() - tw);
       if (!ok) { stop = true; break; }
       const uint32_t cid = *(volatile uint32_t*)&ctl->stage_cid[s];
       if (cid == kSentinel) {

@@ -170,7 +170,7 @@ def get_timeout_ns():
 
 
 PHASE_NAMES = ("epilogue_wait_mma", "row_totals", "lookback", "drain", "producer_wait_stage", "summer",
-               "unused", "tiles")
+               "summer_wait_data", "tiles")
 
 
 def set_phase_profile(enable):
