@@ -77,6 +77,11 @@ TCU_API tcu_status_t tcu_workspace_error(void* ws, uint32_t info[3], int clear, 
  * optionally clear) them with tcu_workspace_phase_ns (synchronises the
  * stream).  Off by default. */
 TCU_API void tcu_set_phase_profile(int enable);
+/* Tuning: CTAs of the persistent scan and compaction launches (0 = one per
+ * SM, the default; smaller values leave SMs to concurrent launches).
+ * Process-wide; the autotuner sets it per size class. */
+TCU_API void tcu_set_max_ctas(int n);
+TCU_API int tcu_get_max_ctas(void);
 TCU_API tcu_status_t tcu_workspace_phase_ns(void* ws, uint64_t out[8], int clear, void* stream);
 
 /* ---- scans ---------------------------------------------------------------

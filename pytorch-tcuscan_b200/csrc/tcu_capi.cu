@@ -16,6 +16,7 @@ namespace tcu {
 static thread_local char g_errmsg[512] = "";
 static uint64_t g_timeout_ns = 4000000000ull;
 static int g_phase_profile = 0;
+static int g_max_ctas = 0;  // 0: one CTA per SM
 
 tcu_status_t cuda_fail(cudaError_t e, const char* what) {
   snprintf(g_errmsg, sizeof(g_errmsg), "%s: %s", what, cudaGetErrorString(e));
@@ -23,6 +24,12 @@ tcu_status_t cuda_fail(cudaError_t e, const char* what) {
 }
 
 uint64_t timeout_ns() { return g_timeout_ns; }
+
+// CTAs of a persistent launch: one per SM, capped by tcu_set_max_ctas.
+int grid_ctas() {
+  const int sms = sm_count();
+  return (g_max_ctas > 0 && g_max_ctas < sms) ? g_max_ctas : sms;
+}
 
 int sm_count() {
   int dev = 0;
@@ -175,7 +182,7 @@ static tcu_status_t launch_scan_tc(const void* x, int64_t n, void* z, double sta
     if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
     attr_set = true;
   }
-  int grid = sm_count();
+  int grid = grid_ctas();
   if (p.num_tiles < grid) grid = (int)p.num_tiles;
   kern<<<grid, kThreads, smem, st>>>(in_map, out_map, p);
   cudaError_t e = cudaGetLastError();
@@ -257,6 +264,8 @@ const char* tcu_status_string(int s) {
 const char* tcu_last_error_message(void) { return g_errmsg; }
 
 void tcu_set_phase_profile(int enable) { g_phase_profile = enable ? 1 : 0; }
+void tcu_set_max_ctas(int n) { g_max_ctas = n > 0 ? n : 0; }
+int tcu_get_max_ctas(void) { return g_max_ctas; }
 
 tcu_status_t tcu_workspace_phase_ns(void* ws, uint64_t out[8], int clear, void* stream) {
   if (!ws) return TCU_ERR_WORKSPACE;

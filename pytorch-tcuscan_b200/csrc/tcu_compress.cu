@@ -532,7 +532,7 @@ static tcu_status_t launch_compress(CompressParams& p, cudaStream_t st) {
     if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(compress)");
     attr_set = true;
   }
-  int grid = sm_count();
+  int grid = grid_ctas();
   if (p.num_tiles < grid) grid = (int)p.num_tiles;
   kern<<<grid, kCmpThreads, C::SMEM, st>>>(mm, xm, im, p);
   cudaError_t e = cudaGetLastError();

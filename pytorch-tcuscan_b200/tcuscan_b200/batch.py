@@ -28,7 +28,7 @@ def scan_rows(x, offsets, S=None, out=None):
         out = torch.empty(n, dtype=tcuscan_ops._scan_out_dtype(x.dtype), device=x.device)
     if n == 0 or offsets.numel() == 0:
         return out
-    S = tcuscan_ops._pick_S(S, x.dtype, n)
+    S = tcuscan_ops._pick_S(S, x.dtype, n, op="seg")
     ws, wsb = tcuscan_ops.workspace(x.device, _lib.lib.tcu_workspace_bytes(n, S))
     st = _lib.lib.tcu_seg_bounds(x.data_ptr(), _lib.DTYPE_CODE[x.dtype], n, S, offsets.data_ptr(),
                                  _lib.DTYPE_CODE[offsets.dtype], offsets.numel(), 0, out.data_ptr(), ws, wsb,

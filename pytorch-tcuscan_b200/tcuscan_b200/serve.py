@@ -440,7 +440,7 @@ class Server:
         ab = self.arena.buf
         st = sl.stream
         sp = ctypes.c_void_p(st.cuda_stream)
-        S = tcuscan_ops._pick_S(self.S, dtype, total)
+        S = tcuscan_ops._pick_S(self.S, dtype, total, op="seg")
         L = _lib.lib
         with torch.cuda.stream(st):
             ab[m_off:m_off + mb].copy_(sl.pinned[:mb], non_blocking=True)
@@ -526,7 +526,7 @@ def one_call_loop(requests, S=None, arrival=None, t0=None):
         if arrival is not None:
             while time.perf_counter() - t0 < arrival[i]:
                 pass
-        s = tcuscan_ops._pick_S(S, x.dtype, x.numel())
+        s = tcuscan_ops._pick_S(S, x.dtype, x.numel(), op="seg" if op == SEG_SUM else "scan")
         if op == SCAN:
             r = tcuscan_ops.run_scan_multi_core(x, s)
         elif op == SEG_SUM:

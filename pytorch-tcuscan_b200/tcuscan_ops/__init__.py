@@ -30,14 +30,20 @@ def _cuda_input(x, name="x"):
     return x
 
 
-def _pick_S(S, dtype, n=None):
-    if S is None or int(S) == 0:
-        from tcuscan_b200 import autotune
+def _pick_S(S, dtype, n=None, op="scan"):
+    """S for a launch: validated when given; from the autotuner's table when
+    None or 0 (which also applies its tuned CTA count; an explicit S runs
+    with one CTA per SM)."""
+    from tcuscan_b200 import autotune
 
-        return autotune.best_S("scan", dtype, n)
+    if S is None or int(S) == 0:
+        S, ctas = autotune.best(op, dtype, n)
+        autotune.apply_ctas(ctas)
+        return S
     S = int(S)
     if S not in _VALID_S:
         raise ValueError(f"S must be one of {_VALID_S} (got {S})")
+    autotune.apply_ctas(0)
     return S
 
 
@@ -198,6 +204,9 @@ def _compress(x, mask, out_len, idx_in=None, idx_mode=0, idx_dtype=torch.int32, 
     elif idx_mode == 2:
         ib = torch.empty((), dtype=idx_dtype).element_size()
     sp = stream_ptr(x.device)
+    from tcuscan_b200 import autotune
+
+    autotune.apply_ctas(autotune.best("compress", x.dtype, n)[1])
     ws, wsb = workspace(x.device, _lib.lib.tcu_workspace_bytes(n, 64))
     counted = out_len is None
     if counted:
@@ -431,7 +440,7 @@ def _seg_scan_flags(x, f, S, ends, where):
     z = torch.empty(n, dtype=_scan_out_dtype(x.dtype), device=x.device)
     if n == 0:
         return z
-    S = _pick_S(S, x.dtype, n)
+    S = _pick_S(S, x.dtype, n, op="seg")
     ws, wsb = workspace(x.device, _lib.lib.tcu_workspace_bytes(n, S))
     st = _lib.lib.tcu_seg_scan(x.data_ptr(), _lib.DTYPE_CODE[x.dtype], n, S, f.data_ptr(), int(ends), z.data_ptr(),
                                ws, wsb, stream_ptr(x.device))
@@ -484,7 +493,7 @@ def _seg_sum_bounds(x, bounds, S, where):
     if nb < 2:
         return out
     n = x.numel()
-    S = _pick_S(S, x.dtype, n)
+    S = _pick_S(S, x.dtype, n, op="seg")
     ws, wsb = workspace(x.device, _lib.lib.tcu_workspace_bytes(n, S))
     st = _lib.lib.tcu_seg_bounds(x.data_ptr(), _lib.DTYPE_CODE[x.dtype], n, S, bounds.data_ptr(),
                                  _lib.DTYPE_CODE[bounds.dtype], nb, 1, out.data_ptr(), ws, wsb, stream_ptr(x.device))
@@ -542,7 +551,7 @@ def run_scan_batch(x, S):
     z = torch.empty((B, L), dtype=_scan_out_dtype(x.dtype), device=x.device)
     if B == 0 or L == 0:
         return z
-    S = _pick_S(S, x.dtype, B * L)
+    S = _pick_S(S, x.dtype, B * L, op="seg")
     ws, wsb = workspace(x.device, _lib.lib.tcu_workspace_bytes(B * L, S))
     st = _lib.lib.tcu_scan_batch(x.data_ptr(), _lib.DTYPE_CODE[x.dtype], B, L, S, z.data_ptr(), ws, wsb,
                                  stream_ptr(x.device))
@@ -572,7 +581,7 @@ def _spmv(vals, indptr, cols, x, S, where):
     if rows <= 0:
         return y
     prod = torch.empty(max(nnz, 4), dtype=torch.float32, device=x.device)
-    S = _pick_S(S, torch.float32, nnz)
+    S = _pick_S(S, torch.float32, nnz, op="seg")
     ws, wsb = workspace(x.device, _lib.lib.tcu_workspace_bytes(nnz, S))
     st = _lib.lib.tcu_spmv_csr(vals.data_ptr(), _lib.DTYPE_CODE[vals.dtype], indptr.data_ptr(),
                                _lib.DTYPE_CODE[indptr.dtype], rows, cols.data_ptr(), nnz, x.data_ptr(), x.numel(), S,

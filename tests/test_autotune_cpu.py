@@ -1,0 +1,91 @@
+"""Autotuner host logic without a GPU: candidates per op and dtype, the
+fastest (S, CTA count) kept, the JSON table written and read back, nearest-
+size lookups, defaults without a table, and the CTA knob reaching the C ABI."""
+import json
+
+import pytest
+import torch
+
+
+@pytest.fixture
+def at(tmp_path, monkeypatch):
+    from tcuscan_b200 import autotune
+
+    monkeypatch.setenv("TCU_AUTOTUNE", "1")
+    autotune.reload(str(tmp_path / "tune.json"))
+    yield autotune
+    autotune.apply_ctas(0)
+    autotune.reload(autotune.CACHE)
+
+
+def _fake(costs):
+    """workload/timer pair: the timed cost is costs(op, dtype, n, S, ctas)."""
+    from tcuscan_ops import _lib
+
+    def workload(op, dtype, n, device):
+        return lambda S: (op, dtype, n, S)
+
+    def timer(fn, steps, warmup):
+        op, dtype, n, S = fn()
+        return costs(op, dtype, n, S, _lib.lib.tcu_get_max_ctas())
+
+    return workload, timer
+
+
+def test_tune_picks_fastest_and_writes_table(at, tmp_path):
+    # S = 64 fastest for scans at 2^20, S = 128 at 2^28; half the SMs best for compress
+    def costs(op, dtype, n, S, ctas):
+        if op == "scan":
+            return abs(S - (64 if n == 1 << 20 else 128)) + 1.0
+        if op == "compress":
+            return 1.0 if ctas == 74 else 2.0
+        return 1.0 + S / 100
+
+    wl, tm = _fake(costs)
+    table = at.tune(device="cpu", ops=("scan", "seg", "compress"), dtypes=(torch.int8, torch.float16),
+                    log2_sizes=(20, 28), workload=wl, timer=tm, path=str(tmp_path / "tune.json"))
+    e = table["entries"]
+    assert e["scan/int8/20"]["S"] == 64 and e["scan/int8/28"]["S"] == 128
+    assert e["scan/float16/20"]["S"] == 64
+    assert e["seg/int8/28"]["S"] == 32
+    assert e["compress/float16/20"]["ctas"] == 74
+    on_disk = json.load(open(tmp_path / "tune.json"))
+    assert on_disk["entries"] == e
+    # lookups, including the nearest tuned size
+    assert at.best("scan", torch.int8, 1 << 20) == (64, 0)
+    assert at.best("scan", torch.int8, 1 << 27) == (128, 0)
+    assert at.best("scan", torch.int8, 1 << 18) == (64, 0)
+    assert at.best("compress", torch.float16, 1 << 21) == (64, 74)
+    assert at.best("scan", torch.float32, 1 << 20) == (64, 0)  # not tuned: default
+
+
+def test_defaults_without_table(at):
+    assert at.best("scan", torch.int8, 1 << 28) == (128, 0)
+    assert at.best("scan", torch.float16, 1 << 28) == (64, 0)
+    assert at.best("seg", torch.float32, 1 << 20) == (64, 0)
+
+
+def test_cta_knob_reaches_library(at):
+    from tcuscan_ops import _lib
+
+    at.apply_ctas(100)
+    assert _lib.lib.tcu_get_max_ctas() == 100
+    at.apply_ctas(0)
+    assert _lib.lib.tcu_get_max_ctas() == 0
+
+
+def test_pick_S_uses_table(at, tmp_path):
+    import tcuscan_ops
+    from tcuscan_ops import _lib
+
+    tab = {"device": "x", "entries": {"scan/int8/24": {"S": 32, "ctas": 120}, "seg/float16/24": {"S": 32, "ctas": 0}}}
+    p = tmp_path / "t2.json"
+    p.write_text(json.dumps(tab))
+    at.reload(str(p))
+    assert tcuscan_ops._pick_S(None, torch.int8, 1 << 24) == 32
+    assert _lib.lib.tcu_get_max_ctas() == 120
+    assert tcuscan_ops._pick_S(64, torch.int8, 1 << 24) == 64  # explicit S: default CTAs
+    assert _lib.lib.tcu_get_max_ctas() == 0
+    assert tcuscan_ops._pick_S(0, torch.float16, 1 << 24, op="seg") == 32
+    with pytest.raises(ValueError):
+        tcuscan_ops._pick_S(48, torch.int8)
