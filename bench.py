@@ -338,6 +338,22 @@ def measure_serving(dev, count=20000, seed=11, sample=240):
     return out
 
 
+def max_over_ranks(value, world, device):
+    """Largest `value` over all ranks (the slowest rank's time); identity on one rank."""
+    if world <= 1:
+        return float(value)
+    import torch
+
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(world, units_per_rank, steps, max_ms):
+    """Whole-job units per second of `world` independent replicas (weak scaling)."""
+    return world * units_per_rank * steps / (max_ms * 1e-3)
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -587,10 +603,7 @@ def main():
     clocks = sampler.summary(wall0, wall1)
     sampler.stop()
 
-    if world > 1:
-        t = torch.tensor([total_ms], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(total_ms, world, dev)
 
     # ---- e2e through the public API with host buffers ----
     x_host = torch.empty(n, dtype=x.dtype, pin_memory=True)
@@ -616,10 +629,7 @@ def main():
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([e2e_ms], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(e2e_ms, world, dev)
 
     extras = None
     if rank == 0 and world == 1 and not args.no_extras:
@@ -642,7 +652,7 @@ def main():
     avg_launch_ms = statistics.mean(per)
     alg_bytes = n * bpe
     achieved = alg_bytes / (avg_launch_ms * 1e-3) / 1e9
-    value = world * n * args.steps / (total_ms * 1e-3)
+    value = replica_throughput(world, n, args.steps, total_ms)
     line = {
         "metric": METRIC,
         "value": value,
@@ -664,7 +674,7 @@ def main():
                      "traffic": profile_traffic(args.op), "algorithmic_bytes_per_launch": alg_bytes,
                      "kernel": "scan_tc_kernel", "avg_launch_ms": avg_launch_ms},
         "cpu_baseline": cpu_base,
-        "e2e": {"value": world * n * e2e_steps / (e2e_ms * 1e-3), "unit": "elem/s",
+        "e2e": {"value": replica_throughput(world, n, e2e_steps, e2e_ms), "unit": "elem/s",
                 "h2d_bytes_per_step": n * x.element_size(), "d2h_bytes_per_step": n * 4,
                 "ms_per_step": e2e_ms / e2e_steps},
         "clocks": clocks,

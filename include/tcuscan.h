@@ -77,6 +77,13 @@ TCU_API tcu_status_t tcu_workspace_error(void* ws, uint32_t info[3], int clear, 
  * optionally clear) them with tcu_workspace_phase_ns (synchronises the
  * stream).  Off by default. */
 TCU_API void tcu_set_phase_profile(int enable);
+/* Self-test of device-side failure detection (no reference counterpart):
+ * one warp waits, with the kernels' own bounded-wait code, on an mbarrier
+ * phase (which = 0) or a look-back descriptor (which = 1) that nothing
+ * completes, gives up after timeout_ns (<= 2 s), records TCU_ERR_TIMEOUT in
+ * `ws` (read it with tcu_workspace_error) and returns.  Nothing faults. */
+TCU_API tcu_status_t tcu_selftest_wait_timeout(int which, uint64_t timeout_ns, void* ws, size_t ws_bytes,
+                                               void* stream);
 /* Tuning: CTAs of the persistent scan and compaction launches (0 = one per
  * SM, the default; smaller values leave SMs to concurrent launches).
  * Process-wide; the autotuner sets it per size class. */

@@ -25,6 +25,37 @@ tcu_status_t cuda_fail(cudaError_t e, const char* what) {
 
 uint64_t timeout_ns() { return g_timeout_ns; }
 
+// Self-test of the bounded waits: one warp waits, with the library's own
+// wait code, on something that nothing will ever complete -- an mbarrier
+// phase (which = 0) or the look-back descriptor of tile 0 (which = 1), read
+// as the look-back of tile 1 does.  The wait gives up after timeout_ns,
+// records TCU_ERR_TIMEOUT with its site in the workspace and the kernel
+// returns; no fault, no trap, and the context stays usable.
+__global__ void selftest_wait_kernel(WsHeader* ws, TileDesc* descs, int which, uint64_t timeout_ns) {
+  __shared__ uint64_t bar;
+  __shared__ int abort_flag;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    abort_flag = 0;
+    fence_mbar_init();
+  }
+  __syncwarp();
+  WaitCtx wc{ws, &abort_flag, timeout_ns};
+  if (which == 0) {
+    if (threadIdx.x == 0) mbar_wait(&bar, 0u, wc, 900, 0);
+  } else {
+    const uint32_t epoch = *(volatile uint32_t*)&ws->epoch;
+    warp_lookback<long long>(1, 0ll, 0, 0ll, descs, epoch, wc, false);
+  }
+  // the look-back published tile 1 under the current epoch: retire the epoch,
+  // as every launch's last CTA does, so the next launch cannot read it
+  __syncwarp();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    atomicAdd(&ws->epoch, 1u);
+  }
+}
+
 // CTAs of a persistent launch: one per SM, capped by tcu_set_max_ctas.
 int grid_ctas() {
   const int sms = sm_count();
@@ -311,6 +342,16 @@ tcu_status_t tcu_workspace_error(void* ws, uint32_t info[3], int clear, void* st
     if (e != cudaSuccess) return cuda_fail(e, "clear workspace error");
   }
   return (tcu_status_t)h.error;
+}
+
+tcu_status_t tcu_selftest_wait_timeout(int which, uint64_t timeout_ns, void* ws, size_t ws_bytes, void* stream) {
+  if (!ws || ws_capacity(ws_bytes) < 2) return TCU_ERR_WORKSPACE;
+  if (which != 0 && which != 1) return TCU_ERR_ARG;
+  if (timeout_ns == 0 || timeout_ns > 2000000000ull) return TCU_ERR_ARG;  // at most 2 s
+  selftest_wait_kernel<<<1, 32, 0, (cudaStream_t)stream>>>(static_cast<WsHeader*>(ws), ws_descs(ws), which,
+                                                           timeout_ns);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? TCU_OK : cuda_fail(e, "selftest_wait_kernel launch");
 }
 
 tcu_status_t tcu_scan(const void* x, tcu_dtype_t x_dtype, int64_t n, int S, double start, void* z, void* ws,
