@@ -466,7 +466,7 @@ def run_profile_op(args, dev):
             nbytes = n * (eb + 4) + bnd.numel() * 8
             sums = 0
         else:
-            steps = torch.empty(n // 64 + 1024, device=dev).geometric_(1 / 64).to(torch.int64)
+            steps = torch.empty(n // args.seg_mean + 1024, device=dev).geometric_(1 / args.seg_mean).to(torch.int64)
             pts = torch.cumsum(steps, 0)
             bnd = torch.cat([torch.zeros(1, dtype=torch.int64, device=dev), pts[pts < n],
                              torch.full((1,), n, dtype=torch.int64, device=dev)])
@@ -522,6 +522,7 @@ def main():
     ap.add_argument("--profile-op", default=None, choices=PROFILE_OPS,
                     help="diagnostics: run only this extra workload (for profiler captures)")
     ap.add_argument("--requests", type=int, default=2000, help="served-stream requests for --profile-op serve")
+    ap.add_argument("--seg-mean", type=int, default=64, help="mean segment length for --profile-op segsum_*")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":

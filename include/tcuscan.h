@@ -149,9 +149,11 @@ TCU_API tcu_status_t tcu_seg_bounds(const void* x, tcu_dtype_t x_dtype, int64_t 
                                     tcu_dtype_t bounds_dtype, int64_t nbounds, int out_sums, void* out, void* ws,
                                     size_t ws_bytes, void* stream);
 /* CSR SpMV y = A x with y fp32: products vals[i] * x[cols[i]] formed in fp32
- * (fp16 products exact) into the caller's prod_tmp (nnz floats, 16-byte
- * aligned), then indptr segment sums on the tensor cores (split-precision
- * bf16 hi + lo, FP64 carries across tiles).  indptr has rows + 1 entries
+ * (fp16 products exact) and written to the caller's prod_tmp (roundup(nnz,
+ * 64) floats, 16-byte aligned) already split into the bf16 hi + lo operand
+ * rows of the tensor-core segmented sum (64 hi then 64 lo per 64 products),
+ * then indptr segment sums on the tensor cores (FP32 accumulation, FP64
+ * carries across tiles).  indptr has rows + 1 entries
  * (int32 or int64).  Replaces run_spmv_v2 (src/torch/torch_spmv.h:112-209),
  * run_spmv_v2_multi_cube (:235-302), run_spmv (:63-94) and
  * run_spmv_multi_cube (:32-46).                                           */

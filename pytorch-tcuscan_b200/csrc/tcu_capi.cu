@@ -141,6 +141,9 @@ struct SegArgs {
   void* seg_out = nullptr;
 };
 
+// Internal input type code (not part of tcu_dtype_t): pre-split fp32 rows.
+constexpr tcu_dtype_t kDtypeSplitF32 = (tcu_dtype_t)100;
+
 template <typename InT, int W, int MODE>
 static tcu_status_t launch_scan_tc(const void* x, int64_t n, void* z, double start_f, long long start_i,
                                    int seg_rows, void* ws, size_t ws_bytes, cudaStream_t st,
@@ -266,6 +269,9 @@ static tcu_status_t dispatch_seg(const void* x, tcu_dtype_t dt, int64_t n, int S
     return launch_scan_tc<__half, 64, MODE>(x, n, z, 0.0, 0, 0, ws, ws_bytes, st, sa);
   }
   if (dt == TCU_FLOAT32) return launch_scan_tc<float, 64, MODE>(x, n, z, 0.0, 0, 0, ws, ws_bytes, st, sa);
+  if constexpr (MODE == kSegBounds) {  // internal: fp32 rows already split into bf16 hi / lo (SpMV products)
+    if (dt == kDtypeSplitF32) return launch_scan_tc<SplitF32, 64, MODE>(x, n, z, 0.0, 0, 0, ws, ws_bytes, st, sa);
+  }
   return TCU_ERR_DTYPE;
 }
 
@@ -416,9 +422,23 @@ tcu_status_t tcu_spmv_csr(const void* vals, tcu_dtype_t dtype, const void* indpt
   if (rows == 0) return TCU_OK;
   if (!y || !indptr || (nnz > 0 && (!prod_tmp || !vals || !cols || !x))) return TCU_ERR_ARG;
   if (nnz > 0 && !aligned16(prod_tmp)) return TCU_ERR_ALIGN;
-  tcu_status_t s = tcu_spmv_products(vals, dtype, cols, nnz, x, x_len, prod_tmp, ws, stream);
+  // products are written already split into the bf16 hi / lo operand rows
+  // of the tensor-core sum, which then needs no conversion pass
+  tcu_status_t s = spmv_products_split(vals, dtype, cols, nnz, x, x_len, prod_tmp, ws, stream);
   if (s != TCU_OK) return s;
-  return tcu_seg_bounds(prod_tmp, TCU_FLOAT32, nnz, S, indptr, indptr_dtype, rows + 1, 1, y, ws, ws_bytes, stream);
+  if (nnz == 0) {
+    cudaError_t e = cudaMemsetAsync(y, 0, (size_t)rows * sizeof(float), (cudaStream_t)stream);
+    return e == cudaSuccess ? TCU_OK : cuda_fail(e, "cudaMemsetAsync(y)");
+  }
+  if (indptr_dtype != TCU_INT32 && indptr_dtype != TCU_INT64) return TCU_ERR_DTYPE;
+  if ((reinterpret_cast<uintptr_t>(indptr) & (indptr_dtype == TCU_INT64 ? 7u : 3u)) != 0) return TCU_ERR_ALIGN;
+  SegArgs sa;
+  sa.bounds = indptr;
+  sa.nbounds = rows + 1;
+  sa.bounds64 = indptr_dtype == TCU_INT64;
+  sa.out_sums = 1;
+  sa.seg_out = y;
+  return dispatch_seg<kSegBounds>(prod_tmp, kDtypeSplitF32, nnz, S, nullptr, sa, ws, ws_bytes, (cudaStream_t)stream);
 }
 
 tcu_status_t tcu_scan_batch(const void* x, tcu_dtype_t x_dtype, int64_t batch, int64_t len, int S, void* z, void* ws,

@@ -19,5 +19,9 @@ bool aligned16(const void* p);
 int64_t ws_capacity(size_t bytes);
 TileDesc* ws_descs(void* ws);
 unsigned long long* ws_phase_counters(void* ws);
+// SpMV products written as pre-split fp32 rows (64 bf16 hi then 64 bf16 lo
+// per 64 products); prod holds roundup(nnz, 64) * 4 bytes.
+tcu_status_t spmv_products_split(const void* values, tcu_dtype_t dtype, const int32_t* cols, int64_t nnz,
+                                 const void* x, int64_t x_len, void* prod, void* ws, void* stream);
 
 }  // namespace tcu

@@ -31,6 +31,15 @@
 
 namespace tcu {
 
+// fp32 input already split into bf16 operands: every 64-element row is
+// stored as 64 bf16 hi = RN(x) then 64 bf16 lo = RN(x - hi) (256 bytes, the
+// size of the fp32 row), so the two TMA boxes of a row land as the hi and lo
+// MMA operand rows and no conversion pass is needed.  Written by the SpMV
+// products kernel.
+struct SplitF32 {
+  uint32_t bits;
+};
+
 enum ScanMode : int {
   kScanFull = 0,     // full inclusive scan with look-back carries (MCSCAN)
   kScanRows = 1,     // per-row (length S) scans only (row_scan)
@@ -84,6 +93,7 @@ template <typename InT, int W, bool SEG = false>
 struct ScanCfg {
   static constexpr int IN_BYTES = (int)sizeof(InT);   // input element bytes
   static constexpr bool IS_F32 = (IN_BYTES == 4);     // fp32: split into bf16 hi + lo operands
+  static constexpr bool PRESPLIT = __is_same(InT, SplitF32);  // ... already split in memory
   static constexpr int ELEM = IS_F32 ? 2 : IN_BYTES;  // MMA operand element bytes
   static constexpr bool IS_INT = (IN_BYTES == 1);
   static constexpr int RB = W * ELEM;                 // operand row bytes
@@ -173,6 +183,17 @@ __device__ __forceinline__ float load_elem<__nv_bfloat16>(const __nv_bfloat16* p
 template <>
 __device__ __forceinline__ float load_elem<float>(const float* p) { return *p; }
 
+// Element e of a 1-D input as float (fp16, fp32 or pre-split fp32 rows).
+template <typename InT>
+__device__ __forceinline__ float load_at(const void* x, int64_t e) {
+  if constexpr (__is_same(InT, SplitF32)) {
+    const __nv_bfloat16* row = static_cast<const __nv_bfloat16*>(x) + (e >> 6) * 128;
+    return __bfloat162float(row[e & 63]) + __bfloat162float(row[64 + (e & 63)]);
+  } else {
+    return load_elem<InT>(static_cast<const InT*>(x) + e);
+  }
+}
+
 // Segmented carry operator on (flag, value): (f1,v1) + (f2,v2) =
 // (f1|f2, f2 ? v2 : v1+v2).  Plain scans only ever use flag = 0.
 template <typename V>
@@ -225,10 +246,36 @@ __device__ __forceinline__ void convert_f32_rows(uint8_t* X0, int term_bytes, in
   __syncwarp();
 }
 
+// Sum of rows [r_lo, vrows) among rows [4 * it_lo, 4 * it_hi) of a
+// pre-split stage (hi rows at X0, lo rows at X0 + term_bytes; the swizzle
+// only permutes 16-byte chunks inside a row, so rows are read as stored).
+__device__ __forceinline__ void sum_split_rows(const uint8_t* X0, int term_bytes, int it_lo, int it_hi, int r_lo,
+                                               int vrows, float& acc) {
+  const int lane = threadIdx.x & 31;
+  const int rr = lane >> 3, cidx = lane & 7;
+#pragma unroll 4
+  for (int it = it_lo; it < it_hi; ++it) {
+    const int row = it * 4 + rr;
+    if (row < vrows && row >= r_lo) {
+      const uint4 h = *reinterpret_cast<const uint4*>(X0 + row * 128 + cidx * 16);
+      const uint4 l = *reinterpret_cast<const uint4*>(X0 + term_bytes + row * 128 + cidx * 16);
+      const __nv_bfloat162* hb = reinterpret_cast<const __nv_bfloat162*>(&h);
+      const __nv_bfloat162* lb = reinterpret_cast<const __nv_bfloat162*>(&l);
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const float2 a = __bfloat1622float2(hb[t]), b = __bfloat1622float2(lb[t]);
+        acc += (a.x + b.x) + (a.y + b.y);
+      }
+    }
+  }
+}
+
 template <typename InT>
 struct OperandT { using T = InT; };
 template <>
 struct OperandT<float> { using T = __nv_bfloat16; };
+template <>
+struct OperandT<SplitF32> { using T = __nv_bfloat16; };
 
 // Build the constant operand B (K-major): row n holds U[k][n] = (k <= n).
 template <typename InT, int W>
@@ -273,10 +320,9 @@ __device__ __forceinline__ void tail_chunk(const ScanParams& p, int col0, uint32
       v[j] = (uint32_t)acci;
     }
   } else {
-    const InT* xs = (const InT*)p.x + base;
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
-      if (col0 + j < p.tail) accf += load_elem<InT>(xs + j);
+      if (col0 + j < p.tail) accf += load_at<InT>(p.x, base + j);
       v[j] = __float_as_uint(accf);
     }
   }
@@ -568,8 +614,8 @@ __device__ __forceinline__ void ctl_publish_seg(const ScanParams& p, uint32_t ti
     const int64_t from = ls > tail0 ? ls : tail0;
     for (int64_t e = from + lane; e < p.n; e += 32) {
       if constexpr (C::IS_INT) acci += (int)static_cast<const int8_t*>(p.x)[e];
-      else if constexpr (C::IS_F32) accd += (double)static_cast<const float*>(p.x)[e];
-      else accf += load_elem<InT>(static_cast<const InT*>(p.x) + e);
+      else if constexpr (C::IS_F32) accd += (double)load_at<InT>(p.x, e);
+      else accf += load_at<InT>(p.x, e);
     }
   }
   V agg;
@@ -643,8 +689,8 @@ __device__ __forceinline__ void scan_summer(const ScanParams& p, uint8_t* smem, 
             const int64_t rend = be0 + (int64_t)(lsr + 1) * W;
             for (int64_t e = ls + lane; e < rend; e += 32) {
               if constexpr (IS_INT) acci += (int)static_cast<const int8_t*>(p.x)[e];
-              else if constexpr (C::IS_F32) accd += (double)static_cast<const float*>(p.x)[e];
-              else accf += load_elem<InT>(static_cast<const InT*>(p.x) + e);
+              else if constexpr (C::IS_F32) accd += (double)load_at<InT>(p.x, e);
+              else accf += load_at<InT>(p.x, e);
             }
           }
         }
@@ -657,7 +703,11 @@ __device__ __forceinline__ void scan_summer(const ScanParams& p, uint8_t* smem, 
         const int64_t vr = p.full_rows - row0;
         const int vrows = vr <= 0 ? 0 : (vr >= 128 ? 128 : (int)vr);
         float acc = 0.f;
-        convert_f32_rows(X0, C::TERM_BYTES, 0, 16, r_lo, vrows, SUMS, acc);
+        if constexpr (C::PRESPLIT) {
+          if (SUMS) sum_split_rows(X0, C::TERM_BYTES, 0, 16, r_lo, vrows, acc);
+        } else {
+          convert_f32_rows(X0, C::TERM_BYTES, 0, 16, r_lo, vrows, SUMS, acc);
+        }
         accd += (double)acc;
         if (lane == 0) mbar_arrive(&ctl->conv[s]);
         if constexpr (SUMS) {  // the other half's sum, stored before its conv arrival
@@ -798,7 +848,11 @@ __device__ __forceinline__ void scan_converter2(const ScanParams& p, uint8_t* sm
         const int64_t vr = p.full_rows - row0;
         const int vrows = vr <= 0 ? 0 : (vr >= 128 ? 128 : (int)vr);
         float acc = 0.f;
-        convert_f32_rows(smem + s * C::STAGE_BYTES, C::TERM_BYTES, 16, 32, r_lo, vrows, SUMS, acc);
+        if constexpr (C::PRESPLIT) {
+          if (SUMS) sum_split_rows(smem + s * C::STAGE_BYTES, C::TERM_BYTES, 16, 32, r_lo, vrows, acc);
+        } else {
+          convert_f32_rows(smem + s * C::STAGE_BYTES, C::TERM_BYTES, 16, 32, r_lo, vrows, SUMS, acc);
+        }
         if constexpr (SUMS) {
           const double t = warp_sum_any((double)acc);
           if (lane == 0) ctl->cv_sum[s] = t;

@@ -119,6 +119,74 @@ __global__ void __launch_bounds__(256) spmv_products_kernel(const T* __restrict_
   }
 }
 
+// The same products, written pre-split for the tensor-core segmented sum:
+// product i goes to row i / 64 of 256 bytes as bf16 hi = RN(p) at column
+// i % 64 and bf16 lo = RN(p - hi) at column 64 + i % 64.  Each thread forms
+// eight consecutive products (one 16-byte store of each half); products past
+// nnz in the last group are written as zero.
+template <typename T>
+__global__ void __launch_bounds__(256) spmv_products_split_kernel(const T* __restrict__ vals,
+                                                                  const int* __restrict__ cols,
+                                                                  const T* __restrict__ x, int64_t nnz, int64_t x_len,
+                                                                  uint8_t* __restrict__ prod, WsHeader* ws) {
+  const int64_t groups = (nnz + 7) / 8;
+  for (int64_t gi = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; gi < groups; gi += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t e0 = gi * 8;
+    float pv[8];
+    if (e0 + 8 <= nnz) {
+      const int4 c0 = __ldg(reinterpret_cast<const int4*>(cols + e0));
+      const int4 c1 = __ldg(reinterpret_cast<const int4*>(cols + e0) + 1);
+      const int cc[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
+      float vv[8];
+      if constexpr (sizeof(T) == 4) {
+        const float4 a = __ldg(reinterpret_cast<const float4*>(vals + e0));
+        const float4 b = __ldg(reinterpret_cast<const float4*>(vals + e0) + 1);
+        vv[0] = a.x; vv[1] = a.y; vv[2] = a.z; vv[3] = a.w; vv[4] = b.x; vv[5] = b.y; vv[6] = b.z; vv[7] = b.w;
+      } else {
+        const uint4 a = __ldg(reinterpret_cast<const uint4*>(vals + e0));
+        const __half2* h = reinterpret_cast<const __half2*>(&a);
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+          const float2 f = __half22float2(h[t]);
+          vv[2 * t] = f.x;
+          vv[2 * t + 1] = f.y;
+        }
+      }
+#pragma unroll
+      for (int t = 0; t < 8; ++t) {
+        float xv = 0.f;
+        if ((unsigned)cc[t] < (unsigned long long)x_len) xv = load_elem<T>(x + cc[t]);
+        else if (ws) record_error(ws, TCU_ERR_ARG, 201, (uint32_t)(e0 + t));
+        pv[t] = __fmul_rn(vv[t], xv);
+      }
+    } else {
+#pragma unroll
+      for (int t = 0; t < 8; ++t) {
+        pv[t] = 0.f;
+        if (e0 + t < nnz) {
+          const int c = __ldg(cols + e0 + t);
+          float xv = 0.f;
+          if ((unsigned)c < (unsigned long long)x_len) xv = load_elem<T>(x + c);
+          else if (ws) record_error(ws, TCU_ERR_ARG, 201, (uint32_t)(e0 + t));
+          pv[t] = __fmul_rn(load_elem<T>(vals + e0 + t), xv);
+        }
+      }
+    }
+    uint32_t hi[4], lo[4];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const __nv_bfloat162 h = __floats2bfloat162_rn(pv[2 * t], pv[2 * t + 1]);
+      const float2 hf = __bfloat1622float2(h);
+      const __nv_bfloat162 l = __floats2bfloat162_rn(pv[2 * t] - hf.x, pv[2 * t + 1] - hf.y);
+      hi[t] = *reinterpret_cast<const uint32_t*>(&h);
+      lo[t] = *reinterpret_cast<const uint32_t*>(&l);
+    }
+    uint8_t* row = prod + (e0 >> 6) * 256 + (e0 & 63) * 2;
+    *reinterpret_cast<uint4*>(row) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+    *reinterpret_cast<uint4*>(row + 128) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // reduce_tiles: block b sums x[b*bl : min((b+1)*bl, n)] with
 // bl = tile_len * ceil(ceil(n / tile_len) / num_blocks)
@@ -351,6 +419,34 @@ tcu_status_t tcu_spmv_products(const void* values, tcu_dtype_t dtype, const int3
     return TCU_ERR_DTYPE;
   return launched("spmv_products");
 }
+
+}  // extern "C"
+
+namespace tcu {
+
+tcu_status_t spmv_products_split(const void* values, tcu_dtype_t dtype, const int32_t* cols, int64_t nnz,
+                                 const void* x, int64_t x_len, void* prod, void* ws, void* stream) {
+  if (nnz < 0 || x_len < 0) return TCU_ERR_ARG;
+  if (nnz == 0) return TCU_OK;
+  if (!values || !cols || !x || !prod) return TCU_ERR_ARG;
+  if (!aligned16(values) || !aligned16(cols) || !aligned16(prod)) return TCU_ERR_ALIGN;
+  cudaStream_t st = (cudaStream_t)stream;
+  WsHeader* h = static_cast<WsHeader*>(ws);
+  const int64_t groups = (nnz + 7) / 8;
+  if (dtype == TCU_FLOAT16)
+    spmv_products_split_kernel<__half><<<grid_for(groups), 256, 0, st>>>((const __half*)values, cols, (const __half*)x,
+                                                                          nnz, x_len, (uint8_t*)prod, h);
+  else if (dtype == TCU_FLOAT32)
+    spmv_products_split_kernel<float><<<grid_for(groups), 256, 0, st>>>((const float*)values, cols, (const float*)x,
+                                                                         nnz, x_len, (uint8_t*)prod, h);
+  else
+    return TCU_ERR_DTYPE;
+  return launched("spmv_products_split");
+}
+
+}  // namespace tcu
+
+extern "C" {
 
 tcu_status_t tcu_reduce_tiles(const void* x, tcu_dtype_t dtype, int64_t n, int64_t tile_len, int num_blocks, void* z,
                               void* ws, size_t ws_bytes, void* stream) {

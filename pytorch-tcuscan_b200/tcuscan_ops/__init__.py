@@ -580,7 +580,7 @@ def _spmv(vals, indptr, cols, x, S, where):
     y = torch.empty(max(rows, 0), dtype=torch.float32, device=x.device)
     if rows <= 0:
         return y
-    prod = torch.empty(max(nnz, 4), dtype=torch.float32, device=x.device)
+    prod = torch.empty(max((nnz + 63) // 64 * 64, 64), dtype=torch.float32, device=x.device)  # pre-split rows
     S = _pick_S(S, torch.float32, nnz, op="seg")
     ws, wsb = workspace(x.device, _lib.lib.tcu_workspace_bytes(nnz, S))
     st = _lib.lib.tcu_spmv_csr(vals.data_ptr(), _lib.DTYPE_CODE[vals.dtype], indptr.data_ptr(),
