@@ -314,25 +314,47 @@ def measure_serving(dev, count=20000, seed=11, sample=240):
     out["poisson_batches"] = int(srv.batches)
     del srv
 
-    # accuracy sample: served in the mix vs single calls
+    # accuracy sample: each request served in the mix and as a single call,
+    # both against an FP64 (int64) reference on the device; integer results
+    # must be identical, floating results are reported as max relative error
+    # with the floor max(|ref|, 1)
     idx = np.sort(np.random.default_rng(seed + 2).choice(count, size=min(sample, count), replace=False))
     srv = serve.Server(dev, budget_bytes=24 << 30, slots=4, keep_results=True)
     srv.submit_many(*wl.arrays(idx), np.zeros(idx.size))
     srv.run()
-    exact_ok, max_rel = True, 0.0
+    exact_ok, err_srv, err_one, diff = True, 0.0, 0.0, 0.0
+
+    def fp64_ref(op, x, aux):
+        if op == serve.SCAN:
+            return torch.cumsum(x.double(), 0)
+        if op == serve.SEG_SUM:
+            lens = (aux[1:] - aux[:-1]).long()
+            rid = torch.repeat_interleave(torch.arange(lens.numel(), device=x.device), lens)
+            return torch.zeros(lens.numel(), dtype=torch.float64, device=x.device).index_add_(0, rid, x.double())
+        return None
+
+    def rel(a, r):
+        return ((a.double() - r).abs() / r.abs().clamp_min(1.0)).max().item() if r.numel() else 0.0
+
     for j, i in enumerate(idx):
         op, x, aux = wl.request(int(i))
         got = srv.result(j)
-        ref = serve.one_call_loop([(op, x, aux)])[0][0]
+        one = serve.one_call_loop([(op, x, aux)])[0][0]
         if x.dtype == torch.int8 or op == serve.COMPRESS:
-            exact_ok &= bool(torch.equal(got, ref))
+            exact_ok &= bool(torch.equal(got, one))
+            if op != serve.COMPRESS:
+                exact_ok &= bool(torch.equal(got.long(), fp64_ref(op, x, aux).long().to(got.dtype).long()))
         else:
-            d = ((got.double() - ref.double()).abs() / ref.double().abs().clamp_min(1.0)).max().item()
-            max_rel = max(max_rel, d)
+            r = fp64_ref(op, x, aux)
+            err_srv = max(err_srv, rel(got, r))
+            err_one = max(err_one, rel(one, r))
+            diff = max(diff, rel(got, one.double()))
     srv.release()
     out["sample_checked"] = int(idx.size)
     out["sample_integer_results_identical"] = exact_ok
-    out["sample_max_rel_diff_float"] = max_rel
+    out["sample_max_rel_err_vs_fp64_served"] = err_srv
+    out["sample_max_rel_err_vs_fp64_single_call"] = err_one
+    out["sample_max_rel_diff_served_vs_single"] = diff
     del wl
     torch.cuda.empty_cache()
     return out

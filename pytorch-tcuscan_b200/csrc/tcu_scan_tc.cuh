@@ -221,7 +221,7 @@ __device__ __forceinline__ void split_bf16x4(const float4 v, uint2& hi, uint2& l
 // operand tiles.  A row is fully read (8 lanes x 2 x 16 B) before any lane
 // writes it.  Rows in [r_lo, vrows) are also summed into acc (FP32 per lane).
 __device__ __forceinline__ void convert_f32_rows(uint8_t* X0, int term_bytes, int it_lo, int it_hi, int r_lo,
-                                                 int vrows, bool sums, float& acc) {
+                                                 int vrows, bool sums, double& acc) {
   uint8_t* X1 = X0 + term_bytes;
   const int lane = threadIdx.x & 31;
   const int rr = lane >> 3, cidx = lane & 7;
@@ -232,7 +232,7 @@ __device__ __forceinline__ void convert_f32_rows(uint8_t* X0, int term_bytes, in
     const float4 a = *reinterpret_cast<const float4*>(X0 + off);
     const float4 b = *reinterpret_cast<const float4*>(X1 + off);
     __syncwarp();
-    if (sums && row < vrows && row >= r_lo) acc += ((a.x + a.y) + (a.z + a.w)) + ((b.x + b.y) + (b.z + b.w));
+    if (sums && row < vrows && row >= r_lo) acc += (double)(((a.x + a.y) + (a.z + a.w)) + ((b.x + b.y) + (b.z + b.w)));
     uint2 ha, la, hb, lb;
     split_bf16x4(a, ha, la);
     split_bf16x4(b, hb, lb);
@@ -250,7 +250,7 @@ __device__ __forceinline__ void convert_f32_rows(uint8_t* X0, int term_bytes, in
 // pre-split stage (hi rows at X0, lo rows at X0 + term_bytes; the swizzle
 // only permutes 16-byte chunks inside a row, so rows are read as stored).
 __device__ __forceinline__ void sum_split_rows(const uint8_t* X0, int term_bytes, int it_lo, int it_hi, int r_lo,
-                                               int vrows, float& acc) {
+                                               int vrows, double& acc) {
   const int lane = threadIdx.x & 31;
   const int rr = lane >> 3, cidx = lane & 7;
 #pragma unroll 4
@@ -261,11 +261,13 @@ __device__ __forceinline__ void sum_split_rows(const uint8_t* X0, int term_bytes
       const uint4 l = *reinterpret_cast<const uint4*>(X0 + term_bytes + row * 128 + cidx * 16);
       const __nv_bfloat162* hb = reinterpret_cast<const __nv_bfloat162*>(&h);
       const __nv_bfloat162* lb = reinterpret_cast<const __nv_bfloat162*>(&l);
+      float t8 = 0.f;
 #pragma unroll
       for (int t = 0; t < 4; ++t) {
         const float2 a = __bfloat1622float2(hb[t]), b = __bfloat1622float2(lb[t]);
-        acc += (a.x + b.x) + (a.y + b.y);
+        t8 += (a.x + b.x) + (a.y + b.y);
       }
+      acc += (double)t8;
     }
   }
 }
@@ -702,13 +704,13 @@ __device__ __forceinline__ void scan_summer(const ScanParams& p, uint8_t* smem, 
         const int64_t row0 = ((int64_t)tid * BPT + j) * 128;
         const int64_t vr = p.full_rows - row0;
         const int vrows = vr <= 0 ? 0 : (vr >= 128 ? 128 : (int)vr);
-        float acc = 0.f;
+        double acc = 0.0;
         if constexpr (C::PRESPLIT) {
           if (SUMS) sum_split_rows(X0, C::TERM_BYTES, 0, 16, r_lo, vrows, acc);
         } else {
           convert_f32_rows(X0, C::TERM_BYTES, 0, 16, r_lo, vrows, SUMS, acc);
         }
-        accd += (double)acc;
+        accd += acc;
         if (lane == 0) mbar_arrive(&ctl->conv[s]);
         if constexpr (SUMS) {  // the other half's sum, stored before its conv arrival
           const bool okc = __all_sync(0xffffffffu, mbar_wait(&ctl->conv[s], (k / C::NSTAGE) & 1u, wc, 9, i));
@@ -721,6 +723,10 @@ __device__ __forceinline__ void scan_summer(const ScanParams& p, uint8_t* smem, 
         int64_t vr = p.full_rows - row0;
         const int vrows = vr <= 0 ? 0 : (vr >= 128 ? 128 : (int)vr);
         const int nv = vrows * (C::SW / 16);
+        // fp16: a stage's values are summed in FP32 in two independent
+        // chains (at most 64 values each per lane) and each stage's partial
+        // goes to the FP64 tile aggregate, which feeds carries across tiles
+        float s0 = 0.f, s1 = 0.f;
 #pragma unroll
         for (int kb = 0; kb < C::KB; ++kb) {
           const uint4* src = (const uint4*)(smem + s * C::STAGE_BYTES + kb * (128 * C::SW));
@@ -733,14 +739,14 @@ __device__ __forceinline__ void scan_summer(const ScanParams& p, uint8_t* smem, 
               acci = __dp4a((int)w.w, 0x01010101, acci);
             } else {
               const __half2* h = reinterpret_cast<const __half2*>(&w);
-#pragma unroll
-              for (int t = 0; t < 4; ++t) {
-                const float2 f = __half22float2(h[t]);
-                accf += f.x + f.y;
-              }
+              const float2 f0 = __half22float2(h[0]), f1 = __half22float2(h[1]);
+              const float2 f2 = __half22float2(h[2]), f3 = __half22float2(h[3]);
+              s0 += (f0.x + f0.y) + (f1.x + f1.y);
+              s1 += (f2.x + f2.y) + (f3.x + f3.y);
             }
           }
         }
+        if constexpr (!IS_INT) accd += (double)(s0 + s1);
       }
       __syncwarp();
       if (lane == 0) mbar_arrive(&ctl->empty[s]);  // this consumer is done with the stage
@@ -847,14 +853,14 @@ __device__ __forceinline__ void scan_converter2(const ScanParams& p, uint8_t* sm
         const int64_t row0 = ((int64_t)tid * BPT + j) * 128;
         const int64_t vr = p.full_rows - row0;
         const int vrows = vr <= 0 ? 0 : (vr >= 128 ? 128 : (int)vr);
-        float acc = 0.f;
+        double acc = 0.0;
         if constexpr (C::PRESPLIT) {
           if (SUMS) sum_split_rows(smem + s * C::STAGE_BYTES, C::TERM_BYTES, 16, 32, r_lo, vrows, acc);
         } else {
           convert_f32_rows(smem + s * C::STAGE_BYTES, C::TERM_BYTES, 16, 32, r_lo, vrows, SUMS, acc);
         }
         if constexpr (SUMS) {
-          const double t = warp_sum_any((double)acc);
+          const double t = warp_sum_any(acc);
           if (lane == 0) ctl->cv_sum[s] = t;
         }
         __syncwarp();
