@@ -230,7 +230,90 @@ def measure_extras(dev, steps=10, warmup=3):
                                        normwise_rel_err_vs_fp64=err_norm, max_rel_err_vs_fp64=err_el,
                                        launch="one CUDA-graph replay per step")
     del xr, zr, cs, base, refr, seg_start
+
+    # small fp16 scan (n = 2^20, S = 64, values uniform[-1, 1)): latency-bound;
+    # one call end to end on the host (launch included) and the kernel alone
+    # replayed from a CUDA graph
+    import time as _t
+
+    n20 = 1 << 20
+    x20 = workloads.scan_input(n20, torch.float16, dev, seed=0)
+    for _ in range(20):
+        tcuscan_ops.run_scan_single_core(x20, 64)
+    torch.cuda.synchronize()
+    t0 = _t.perf_counter()
+    for _ in range(200):
+        tcuscan_ops.run_scan_single_core(x20, 64)
+        torch.cuda.synchronize()
+    call_us = (_t.perf_counter() - t0) / 200 * 1e6
+    g20 = torch.cuda.CUDAGraph()
+    st20 = torch.cuda.Stream(dev)
+    st20.wait_stream(torch.cuda.current_stream(dev))
+    with torch.cuda.stream(st20):
+        tcuscan_ops.run_scan_single_core(x20, 64)  # workspace of this stream exists before capture
+        torch.cuda.synchronize()
+        with torch.cuda.graph(g20, stream=st20):
+            z20 = tcuscan_ops.run_scan_single_core(x20, 64)
+    ms20 = _device_ms(g20.replay, 50, 5)
+    ref20 = torch.cumsum(x20.double(), 0)
+    err20 = ((z20.double() - ref20).abs() / ref20.abs().clamp_min(1.0)).max().item()
+    out["scan_f16_2e20"] = entry(n20, 6 * n20, ms20, S=64, host_call_us=call_us, max_rel_err_vs_fp64=err20,
+                                 note="kernel time from CUDA-graph replays; host_call_us = one synchronised call")
+    del g20, x20, z20, ref20
     torch.cuda.empty_cache()
+    return out
+
+
+def cpu_baselines_other(seed=0):
+    """Host-core baselines for the ops without a reference CPU implementation
+    (bounded samples): compaction with torch.masked_select, indptr segment
+    sums with numpy add.reduceat, CSR SpMV with SciPy, all on the host's cores."""
+    import numpy as np
+    import torch
+
+    out = {}
+    rng = np.random.default_rng(seed)
+    n = 1 << 24
+    x = torch.from_numpy(rng.standard_normal(n).astype(np.float16))
+    m = torch.from_numpy(rng.random(n) < 0.3)
+    torch.masked_select(x, m)
+    t0 = time.perf_counter()
+    for _ in range(5):
+        torch.masked_select(x, m)
+    dt = (time.perf_counter() - t0) / 5
+    out["compress_f16_masked_select"] = {"value": n / dt, "unit": "elem/s", "cores": torch.get_num_threads(),
+                                         "kind": "torch", "sample": "2^24 fp16, Bernoulli(0.3) mask, 5 runs"}
+    lens = rng.geometric(1 / 64, size=n // 64)
+    idx = np.concatenate([[0], np.cumsum(lens)])
+    idx = idx[idx < n]
+    xf = rng.standard_normal(n).astype(np.float32)
+    np.add.reduceat(xf, idx)
+    t0 = time.perf_counter()
+    for _ in range(5):
+        np.add.reduceat(xf, idx)
+    dt = (time.perf_counter() - t0) / 5
+    out["seg_sum_f32_reduceat"] = {"value": n / dt, "unit": "elem/s", "cores": 1, "kind": "numpy",
+                                   "sample": "2^24 fp32, geometric(mean 64) segments, 5 runs"}
+    try:
+        from scipy.sparse import csr_matrix
+
+        from tcuscan_b200 import workloads
+
+        lens = workloads.zipf_row_lengths(1 << 20, target_nnz=1 << 22, seed=9)
+        indptr = np.concatenate([[0], np.cumsum(lens)])
+        nnz = int(indptr[-1])
+        A = csr_matrix((rng.standard_normal(nnz).astype(np.float32), rng.integers(0, 1 << 20, nnz), indptr),
+                       shape=(1 << 20, 1 << 20))
+        xv = rng.uniform(-1, 1, 1 << 20).astype(np.float32)
+        A @ xv
+        t0 = time.perf_counter()
+        for _ in range(5):
+            A @ xv
+        dt = (time.perf_counter() - t0) / 5
+        out["spmv_f32_scipy"] = {"value": nnz / dt, "unit": "nnz/s", "cores": 1, "kind": "scipy",
+                                 "sample": f"2^20 x 2^20 Zipf(1.6) rows, {nnz} nnz, 5 runs"}
+    except ImportError:  # pragma: no cover
+        pass
     return out
 
 
@@ -659,6 +742,8 @@ def main():
         del x_host, z_host, x_dev
         extras = measure_extras(dev)
         extras["served_stream"] = measure_serving(dev)
+        if not args.no_cpu:
+            extras["cpu_baselines_other_ops"] = cpu_baselines_other()
 
     cpu_base = None
     if rank == 0 and world == 1 and not args.no_cpu:

@@ -75,6 +75,31 @@ __global__ void __launch_bounds__(256) pack_kernel(const tcu_pack_item_t* __rest
     }
     __syncthreads();
     const int64_t lo = s_range[0], hi = s_range[1];
+    if (lo == hi && SB == DB) {
+      // the whole chunk lies in one item: one item read, then all of this
+      // thread's 16-byte loads in flight before its stores
+      const tcu_pack_item_t it = items[lo];
+      const int64_t a = c0 - it.dst;
+      const uintptr_t sa = reinterpret_cast<uintptr_t>(it.src) + (uintptr_t)(a * SB);
+      if (a >= 0 && c1 - it.dst <= it.n && (sa & 15u) == 0 && it.add == 0 && ((c1 - c0) % VEC) == 0) {
+        const uint4* src = reinterpret_cast<const uint4*>(sa);
+        uint4* out = reinterpret_cast<uint4*>(dst + c0 * DB);
+        const int nv = (int)((c1 - c0) / VEC);
+        uint4 r[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const int vi = k * 256 + threadIdx.x;
+          if (vi < nv) r[k] = __ldg(src + vi);
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const int vi = k * 256 + threadIdx.x;
+          if (vi < nv) out[vi] = r[k];
+        }
+        __syncthreads();  // s_range is rewritten for the next chunk
+        continue;
+      }
+    }
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
       const int64_t d0 = c0 + ((int64_t)k * 256 + threadIdx.x) * VEC;

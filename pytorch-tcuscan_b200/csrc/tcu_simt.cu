@@ -152,12 +152,21 @@ __global__ void __launch_bounds__(256) spmv_products_split_kernel(const T* __res
           vv[2 * t + 1] = f.y;
         }
       }
+      // all eight gathers are issued before any is used (an out-of-range
+      // column reads x[0] and is replaced by zero and reported afterwards)
+      float xg[8];
+      bool okc[8];
 #pragma unroll
       for (int t = 0; t < 8; ++t) {
-        float xv = 0.f;
-        if ((unsigned)cc[t] < (unsigned long long)x_len) xv = load_elem<T>(x + cc[t]);
-        else if (ws) record_error(ws, TCU_ERR_ARG, 201, (uint32_t)(e0 + t));
-        pv[t] = __fmul_rn(vv[t], xv);
+        okc[t] = (unsigned long long)(unsigned)cc[t] < (unsigned long long)x_len;
+        xg[t] = load_elem<T>(x + (okc[t] ? cc[t] : 0));
+      }
+#pragma unroll
+      for (int t = 0; t < 8; ++t) pv[t] = __fmul_rn(vv[t], okc[t] ? xg[t] : 0.f);
+      if (ws) {
+#pragma unroll
+        for (int t = 0; t < 8; ++t)
+          if (!okc[t]) record_error(ws, TCU_ERR_ARG, 201, (uint32_t)(e0 + t));
       }
     } else {
 #pragma unroll
