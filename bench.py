@@ -190,7 +190,17 @@ def measure_extras(dev, steps=10, warmup=3):
     xv = torch.randn(n, device=dev).half()
     ms = _device_ms(lambda: tcuscan_ops.run_compress_ind_no_arange(xv, mask, 64), 3, 1)
     out["compress_ind_no_arange_f16_incl_count_sync"] = entry(n, n * 3 + k * 6, ms, selected=k)
-    del xv, mask
+    ar = torch.arange(n, dtype=torch.int32, device=dev)
+    ms = _device_ms(lambda: tcuscan_ops.run_compress_ind(xv, ar, mask, 64), 3, 1)
+    out["compress_ind_f16_arange_incl_count_sync"] = entry(n, n * 7 + k * 6, ms, selected=k)
+    del xv, mask, ar
+
+    # flag-driven segmented scan (starts), fp16 2^28, flags Bernoulli(0.01)
+    xf = workloads.scan_input(n, torch.float16, dev, seed=12)
+    fl = workloads.bernoulli_mask(n, 0.01, dev, seed=13)
+    ms = _device_ms(lambda: tcuscan_ops.run_seg_scan(xf, fl, 64), steps, warmup)
+    out["seg_scan_flags_f16_2e28"] = entry(n, n * (2 + 1 + 4), ms)
+    del xf, fl
 
     # CSR SpMV (products + indptr segment sums)
     for name, dt in (("spmv_f32", torch.float32), ("spmv_f16", torch.float16)):
@@ -210,6 +220,12 @@ def measure_extras(dev, steps=10, warmup=3):
         bytes_ = nnz * (eb + 4) + (rows + 1) * 4 + rows * 4 + xs.numel() * eb
         out[name] = entry(nnz, bytes_, ms, unit="nnz/s", rows=rows, nnz=nnz, max_rel_err_vs_fp64=err,
                           kernels=2)
+        if dt == torch.float32:  # the segment sums alone, on fp32 products with the same row pointers
+            prod = (vals * xs[cols.long()]).contiguous()
+            ms = _device_ms(lambda: tcuscan_ops.run_seg_sum_multi_core(prod, indptr, 64), steps, warmup)
+            out["seg_sum_f32_spmv_rows"] = entry(nnz, nnz * 4 + (rows + 1) * 4 + rows * 4, ms, unit="nnz/s",
+                                                 rows=rows)
+            del prod
         del vals, indptr, cols, xs, y
 
     # 4096 uneven fp32 rows, one CUDA-graph launch
@@ -787,6 +803,7 @@ def main():
                 "ms_per_step": e2e_ms / e2e_steps},
         "clocks": clocks,
         "gpu_launches": args.steps,
+        "median_ms_per_launch": statistics.median(per),
         "extras": extras,
     }
     print(json.dumps(line), flush=True)

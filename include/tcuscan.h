@@ -214,6 +214,14 @@ TCU_API tcu_status_t tcu_mask_count(const int8_t* mask, int64_t n, void* count_d
 TCU_API tcu_status_t tcu_csr_gather(const void* values, tcu_dtype_t dtype, const int32_t* cols, int64_t nnz,
                                     const void* x, int64_t x_len, void* z, void* ws, void* stream);
 
+/* z[i] = values[idxs[i] - 1] (elements of 2, 4 or 8 bytes), 0 where
+ * idxs[i] == 0; idxs int32 / uint32 / int64.  An index past the values is
+ * recorded in `ws` (if given) and gives 0.  Replaces run_gather_spmv
+ * (src/torch/torch_gather.h:182-213), the row-pointer gather of the
+ * reference's v1 SpMV.                                                     */
+TCU_API tcu_status_t tcu_gather_spmv(const void* values, int elem_bytes, int64_t n_values, const void* idxs,
+                                     tcu_dtype_t idx_dtype, int64_t n_idx, void* z, void* ws, void* stream);
+
 /* ---- scan phases as standalone operators ----------------------------------
  * reduce_tiles: z[b] = sum of block b, block = tile_len * ceil(ceil(n /
  * tile_len) / num_blocks) elements; int8 -> int32, fp16 -> fp32.  Needs

@@ -196,6 +196,35 @@ __global__ void __launch_bounds__(256) spmv_products_split_kernel(const T* __res
   }
 }
 
+// gather_spmv (tests/test_gather_spmv.py): z[i] = values[idxs[i] - 1], and 0
+// where idxs[i] == 0 -- the scanned products read back at the row pointers
+// (the first step of the reference's v1 SpMV, src/torch/torch_spmv.h:79-93).
+// Indices past the values are reported (site 202) and read as 0.
+template <int EB, typename I>
+__global__ void __launch_bounds__(256) gather_spmv_kernel(const uint8_t* __restrict__ values, int64_t n_values,
+                                                          const I* __restrict__ idxs, int64_t n_idx,
+                                                          uint8_t* __restrict__ z, WsHeader* ws) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n_idx; i += (int64_t)gridDim.x * blockDim.x) {
+    const unsigned long long k = (unsigned long long)__ldg(idxs + i);
+    uint32_t lo = 0, hi = 0;
+    if (k >= 1 && k - 1 < (unsigned long long)n_values) {
+      const uint8_t* src = values + (k - 1) * EB;
+      if constexpr (EB == 2) lo = __ldg(reinterpret_cast<const uint16_t*>(src));
+      if constexpr (EB == 4) lo = __ldg(reinterpret_cast<const uint32_t*>(src));
+      if constexpr (EB == 8) {
+        const unsigned long long v = __ldg(reinterpret_cast<const unsigned long long*>(src));
+        lo = (uint32_t)v;
+        hi = (uint32_t)(v >> 32);
+      }
+    } else if (k != 0 && ws) {
+      record_error(ws, TCU_ERR_ARG, 202, (uint32_t)i);
+    }
+    if constexpr (EB == 2) reinterpret_cast<uint16_t*>(z)[i] = (uint16_t)lo;
+    if constexpr (EB == 4) reinterpret_cast<uint32_t*>(z)[i] = lo;
+    if constexpr (EB == 8) reinterpret_cast<unsigned long long*>(z)[i] = ((unsigned long long)hi << 32) | lo;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // reduce_tiles: block b sums x[b*bl : min((b+1)*bl, n)] with
 // bl = tile_len * ceil(ceil(n / tile_len) / num_blocks)
@@ -456,6 +485,29 @@ tcu_status_t spmv_products_split(const void* values, tcu_dtype_t dtype, const in
 }  // namespace tcu
 
 extern "C" {
+
+tcu_status_t tcu_gather_spmv(const void* values, int elem_bytes, int64_t n_values, const void* idxs,
+                             tcu_dtype_t idx_dtype, int64_t n_idx, void* z, void* ws, void* stream) {
+  if (n_values < 0 || n_idx < 0) return TCU_ERR_ARG;
+  if (n_idx == 0) return TCU_OK;
+  if (!idxs || !z || (n_values > 0 && !values)) return TCU_ERR_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  WsHeader* h = static_cast<WsHeader*>(ws);
+  const uint8_t* v = static_cast<const uint8_t*>(values);
+  uint8_t* zo = static_cast<uint8_t*>(z);
+  const int grid = grid_for(n_idx);
+#define TCU_GS(EB, I) gather_spmv_kernel<EB, I><<<grid, 256, 0, st>>>(v, n_values, (const I*)idxs, n_idx, zo, h)
+  const bool i32 = idx_dtype == TCU_INT32 || idx_dtype == TCU_UINT32;
+  if (!i32 && idx_dtype != TCU_INT64) return TCU_ERR_DTYPE;
+  switch (elem_bytes) {
+    case 2: if (i32) TCU_GS(2, uint32_t); else TCU_GS(2, unsigned long long); break;
+    case 4: if (i32) TCU_GS(4, uint32_t); else TCU_GS(4, unsigned long long); break;
+    case 8: if (i32) TCU_GS(8, uint32_t); else TCU_GS(8, unsigned long long); break;
+    default: return TCU_ERR_DTYPE;
+  }
+#undef TCU_GS
+  return launched("gather_spmv");
+}
 
 tcu_status_t tcu_reduce_tiles(const void* x, tcu_dtype_t dtype, int64_t n, int64_t tile_len, int num_blocks, void* z,
                               void* ws, size_t ws_bytes, void* stream) {

@@ -345,6 +345,30 @@ def run_csr_gather(values, cols, x):
 # ---------------------------------------------------------------------------
 # scan phases as standalone operators (src/torch/torch_reduce.h)
 
+def run_gather_spmv(values, idxs, tile_len):
+    """z[i] = values[idxs[i] - 1], 0 where idxs[i] == 0 (reference:
+    src/torch/torch_gather.h:182-213; tests/test_gather_spmv.py).  Output has
+    len(idxs) elements of the values dtype.  tile_len is the reference's
+    vector-core tile and is validated but not needed here."""
+    if int(tile_len) <= 0:
+        raise ValueError("tile_len must be positive")
+    values = _cuda_input(values, "values")
+    idxs = _cuda_input(idxs, "idxs")
+    if values.element_size() not in (2, 4, 8):
+        raise TypeError(f"run_gather_spmv: unsupported values dtype {values.dtype}")
+    code = _lib.DTYPE_CODE.get(idxs.dtype)
+    if code not in (_lib.TCU_INT32, _lib.TCU_INT64, _lib.TCU_UINT32):
+        raise TypeError(f"run_gather_spmv: indices must be int32, uint32 or int64, got {idxs.dtype}")
+    z = torch.empty(idxs.numel(), dtype=values.dtype, device=values.device)
+    if idxs.numel() == 0:
+        return z
+    ws, _ = workspace(values.device, 1 << 20)
+    check(_lib.lib.tcu_gather_spmv(values.data_ptr(), values.element_size(), values.numel(), idxs.data_ptr(), code,
+                                   idxs.numel(), z.data_ptr(), ws, stream_ptr(values.device)), "run_gather_spmv")
+    _after(values)
+    return z
+
+
 def run_reduce_tiles(x, tile_len, num_blocks):
     """Per-block sums (reference: src/torch/torch_reduce.h:42-75):
     block = tile_len * ceil(ceil(n / tile_len) / num_blocks) elements;

@@ -80,6 +80,7 @@ _sig("tcu_compress_counted", _ST, _P, _I, _P, _I64, _P, _I, _I, _P, _P, _I64, _P
 _sig("tcu_compress_segments", _ST, _P, _I, _P, _I64, _P, _I64, _P, _I64, _P, _P, _SZ, _P)
 _sig("tcu_pack", _ST, _P, _I64, _I, _I, _P, _I64, _P)
 _sig("tcu_csr_gather", _ST, _P, _I, _P, _I64, _P, _I64, _P, _P, _P)
+_sig("tcu_gather_spmv", _ST, _P, _I, _I64, _P, _I, _I64, _P, _P, _P)
 _sig("tcu_reduce_tiles", _ST, _P, _I, _I64, _I64, _I, _P, _P, _SZ, _P)
 _sig("tcu_complete_rows", _ST, _P, _I, _I64, _P, _I, _I64, _P, _P, _SZ, _P)
 _sig("tcu_complete_blocks", _ST, _P, _I, _I64, _P, _I, _P, _P)

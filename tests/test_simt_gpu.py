@@ -179,3 +179,47 @@ def test_gen_lower(s, dtype):
 
     z = tcuscan_ops.run_gen_lower(s, torch.device(DEV), dtype)
     assert torch.equal(z, torch.tril(torch.ones((s, s), dtype=dtype, device=DEV)))
+
+
+# ---- gather_spmv (the row-pointer gather of the v1 SpMV) -----------------------
+@pytest.mark.parametrize("offset", [0, 7, 17])
+@pytest.mark.parametrize("multiplier", [1, 4, 15])
+@pytest.mark.parametrize("s", [64, 128])
+def test_gather_spmv_reference_grid(offset, multiplier, s):
+    """Grid of the reference test (tests/test_gather_spmv.py): nnz = m*20*s*s
+    fp32 values, s*s - offset sorted uint32 indices in [0, nnz); exact."""
+    import tcuscan_ops
+
+    nnz = multiplier * 20 * s * s
+    n_idx = s * s - offset
+    rng = np.random.default_rng(nnz + n_idx)
+    vals = rng.uniform(1, 100, nnz).astype(np.float32)
+    idx = np.sort(rng.uniform(0, nnz, n_idx)).astype(np.uint32)
+    expect = np.where(idx >= 1, vals[np.maximum(idx.astype(np.int64) - 1, 0)], 0).astype(np.float32)
+    got = tcuscan_ops.run_gather_spmv(torch.from_numpy(vals).to(DEV), torch.from_numpy(idx).to(DEV), s)
+    assert got.dtype == torch.float32 and got.shape == (n_idx,)
+    assert np.array_equal(got.cpu().numpy(), expect)
+
+
+@pytest.mark.parametrize("vdtype", [torch.float16, torch.float32, torch.float64])
+@pytest.mark.parametrize("idtype", [torch.int32, torch.int64])
+def test_gather_spmv_dtypes_and_v1_spmv(vdtype, idtype):
+    """Other dtypes, and the reference's v1 SpMV built from the pieces:
+    diff(gather_spmv(scan(products), indptr)) equals the row sums."""
+    import tcuscan_ops
+
+    rng = np.random.default_rng(3)
+    n = 50_000
+    vals = torch.from_numpy(rng.standard_normal(n)).to(vdtype)
+    idx = torch.from_numpy(np.sort(rng.integers(0, n + 1, 4000))).to(idtype)
+    got = tcuscan_ops.run_gather_spmv(vals.to(DEV), idx.to(DEV), 128).cpu()
+    ref = torch.where(idx >= 1, vals[(idx - 1).clamp_min(0)], torch.zeros((), dtype=vdtype))
+    assert torch.equal(got, ref)
+    # v1 SpMV composition on fp32 products
+    lens = rng.integers(0, 40, 3000)
+    indptr = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+    prod = rng.standard_normal(int(indptr[-1])).astype(np.float32)
+    scanned = tcuscan_ops.run_scan_multi_core(torch.from_numpy(prod).to(DEV), 64)
+    rows = torch.diff(tcuscan_ops.run_gather_spmv(scanned, torch.from_numpy(indptr).to(DEV), 128)).cpu().numpy()
+    ref_rows = oracle.seg_sum_indptr(prod, indptr.astype(np.int64))
+    assert oracle.max_rel_err(rows, ref_rows, floor=float(np.abs(np.cumsum(prod.astype(np.float64))).max())) <= 1e-4
