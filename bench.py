@@ -1,12 +1,14 @@
 """Benchmark of the tensor-core scan family on B200 (one JSON line on rank 0).
 
-Headline workload: int8 1-D inclusive scan, n = 2^28 -> int32 (S = 64), one
-persistent tcgen05 launch per step.  ``value`` is whole-job elements/s with
-the input resident in HBM (device time, CUDA events, max over ranks);
-``e2e`` is the same metric through ``tcuscan_ops.run_scan_multi_core`` with
-the input copied from pinned host memory and the full result read back every
-step.  The input (256 MiB) and output (1 GiB) are larger than L2 (126 MB), so
-no explicit flush is needed between steps.
+Headline workload: int8 1-D inclusive scan, n = 2^28 -> int32 (S autotuned:
+128), one persistent tcgen05 launch per step.  ``value`` is whole-job
+elements/s with the input resident in HBM (device time, CUDA events, max over
+ranks); ``e2e`` is the same metric through the host-buffer scan
+(``tcuscan_b200.stream``: the input copied from pinned host memory and the
+full result read back every step, chunk by chunk on three streams so the two
+copy directions and the scans overlap).  The input (256 MiB) and output
+(1 GiB) are larger than L2 (126 MB), so no explicit flush is needed between
+steps.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--op scan_i8|scan_f16]
     python bench.py --impl reference ...   # the reference CPU scan on host cores
@@ -727,21 +729,32 @@ def main():
 
     total_ms = max_over_ranks(total_ms, world, dev)
 
-    # ---- e2e through the public API with host buffers ----
+    # ---- e2e through the public API with host buffers: the host-buffer scan
+    # (tcuscan_b200.stream) copies each 2^24-element chunk in, scans it and
+    # copies it out on three streams, the chunks chained on the device ----
+    from tcuscan_b200 import stream as host_stream
+
     x_host = torch.empty(n, dtype=x.dtype, pin_memory=True)
     x_host.copy_(x.cpu())
     out_dtype = torch.int32 if dname == "int8" else torch.float32
     z_host = torch.empty(n, dtype=out_dtype, pin_memory=True)
-    x_dev = torch.empty_like(x)
+    scanner = host_stream.HostScanner(n, x.dtype, dev, chunk=1 << 24)
     e2e_steps = max(3, min(args.steps, 20))
 
     def e2e_step():
-        x_dev.copy_(x_host, non_blocking=True)
-        z = tcuscan_ops.run_scan_multi_core(x_dev, args.S)
-        z_host.copy_(z, non_blocking=True)
+        scanner.scan(x_host, z_host, args.S)
 
     e2e_step()
     torch.cuda.synchronize()
+    # the host result ends with the total of the input (int32 wrap for int8)
+    if dname == "int8":
+        tot = int(x.long().sum().item())
+        ok = int(z_host[-1].item()) == ((tot + 2 ** 31) % 2 ** 32) - 2 ** 31
+    else:
+        tot = float(x.double().sum().item())
+        ok = abs(float(z_host[-1].item()) - tot) <= 1e-3 * max(1.0, abs(tot))
+    if not ok:
+        raise RuntimeError("end-to-end scan result differs from the input total")
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     if world > 1:
         torch.distributed.barrier()
@@ -755,7 +768,7 @@ def main():
 
     extras = None
     if rank == 0 and world == 1 and not args.no_extras:
-        del x_host, z_host, x_dev
+        del x_host, z_host, scanner
         extras = measure_extras(dev)
         extras["served_stream"] = measure_serving(dev)
         if not args.no_cpu:

@@ -104,6 +104,15 @@ TCU_API tcu_status_t tcu_workspace_phase_ns(void* ws, uint64_t out[8], int clear
 TCU_API tcu_status_t tcu_scan(const void* x, tcu_dtype_t x_dtype, int64_t n, int S, double start, void* z, void* ws,
                       size_t ws_bytes, void* stream);
 
+/* tcu_scan whose starting value also includes one element read from device
+ * memory when the kernel runs (start_dev: int32 for int8 inputs, fp32
+ * otherwise; NULL = none).  Chunks of a long input scanned one after another
+ * on one stream, each given the previous chunk's last output as start_dev,
+ * give the scan of the whole input without a host round trip between them
+ * (used to overlap host copies with the scan, tcuscan_b200.stream).        */
+TCU_API tcu_status_t tcu_scan_chained(const void* x, tcu_dtype_t x_dtype, int64_t n, int S, double start,
+                                      const void* start_dev, void* z, void* ws, size_t ws_bytes, void* stream);
+
 /* Inclusive scan that allocates nothing.  No counterpart in the reference.
  * Same arguments and results as tcu_scan, minus the workspace, for callers
  * that cannot allocate device memory where they scan (inside an allocator or

@@ -147,7 +147,7 @@ constexpr tcu_dtype_t kDtypeSplitF32 = (tcu_dtype_t)100;
 template <typename InT, int W, int MODE>
 static tcu_status_t launch_scan_tc(const void* x, int64_t n, void* z, double start_f, long long start_i,
                                    int seg_rows, void* ws, size_t ws_bytes, cudaStream_t st,
-                                   const SegArgs& sa = SegArgs()) {
+                                   const SegArgs& sa = SegArgs(), const void* start_dev = nullptr) {
   using C = ScanCfg<InT, W, is_seg(MODE)>;
   ScanParams p{};
   p.x = x;
@@ -161,6 +161,7 @@ static tcu_status_t launch_scan_tc(const void* x, int64_t n, void* z, double sta
   p.num_tiles = (total_rows + tile_rows - 1) / tile_rows;
   p.start_f = start_f;
   p.start_i = start_i;
+  p.start_dev = start_dev;
   p.timeout_ns = g_timeout_ns;
   if (ws == nullptr || ws_capacity(ws_bytes) < p.num_tiles) {
     snprintf(g_errmsg, sizeof(g_errmsg), "workspace too small: %lld tiles need %zu bytes", (long long)p.num_tiles,
@@ -230,26 +231,26 @@ static tcu_status_t launch_scan_tc(const void* x, int64_t n, void* z, double sta
 
 template <int MODE>
 static tcu_status_t dispatch_scan(const void* x, tcu_dtype_t dt, int64_t n, int S, void* z, double start, int seg_rows,
-                                  void* ws, size_t ws_bytes, cudaStream_t st) {
+                                  void* ws, size_t ws_bytes, cudaStream_t st, const void* start_dev = nullptr) {
   const long long si = (long long)start;
   if (dt == TCU_INT8) {
     switch (S) {
-      case 32: return launch_scan_tc<int8_t, 32, MODE>(x, n, z, 0.0, si, seg_rows, ws, ws_bytes, st);
-      case 64: return launch_scan_tc<int8_t, 64, MODE>(x, n, z, 0.0, si, seg_rows, ws, ws_bytes, st);
-      case 128: return launch_scan_tc<int8_t, 128, MODE>(x, n, z, 0.0, si, seg_rows, ws, ws_bytes, st);
+      case 32: return launch_scan_tc<int8_t, 32, MODE>(x, n, z, 0.0, si, seg_rows, ws, ws_bytes, st, SegArgs(), start_dev);
+      case 64: return launch_scan_tc<int8_t, 64, MODE>(x, n, z, 0.0, si, seg_rows, ws, ws_bytes, st, SegArgs(), start_dev);
+      case 128: return launch_scan_tc<int8_t, 128, MODE>(x, n, z, 0.0, si, seg_rows, ws, ws_bytes, st, SegArgs(), start_dev);
       default: return TCU_ERR_ARG;
     }
   }
   if (dt == TCU_FLOAT32) {  // split-precision bf16 hi + lo operands, 64-column rows
     if (MODE != kScanFull) return TCU_ERR_DTYPE;
-    return launch_scan_tc<float, 64, kScanFull>(x, n, z, start, 0, seg_rows, ws, ws_bytes, st);
+    return launch_scan_tc<float, 64, kScanFull>(x, n, z, start, 0, seg_rows, ws, ws_bytes, st, SegArgs(), start_dev);
   }
   if (dt == TCU_FLOAT16) {
     switch (S) {
-      case 16: return launch_scan_tc<__half, 16, MODE>(x, n, z, start, 0, seg_rows, ws, ws_bytes, st);
-      case 32: return launch_scan_tc<__half, 32, MODE>(x, n, z, start, 0, seg_rows, ws, ws_bytes, st);
-      case 64: return launch_scan_tc<__half, 64, MODE>(x, n, z, start, 0, seg_rows, ws, ws_bytes, st);
-      case 128: return launch_scan_tc<__half, 128, MODE>(x, n, z, start, 0, seg_rows, ws, ws_bytes, st);
+      case 16: return launch_scan_tc<__half, 16, MODE>(x, n, z, start, 0, seg_rows, ws, ws_bytes, st, SegArgs(), start_dev);
+      case 32: return launch_scan_tc<__half, 32, MODE>(x, n, z, start, 0, seg_rows, ws, ws_bytes, st, SegArgs(), start_dev);
+      case 64: return launch_scan_tc<__half, 64, MODE>(x, n, z, start, 0, seg_rows, ws, ws_bytes, st, SegArgs(), start_dev);
+      case 128: return launch_scan_tc<__half, 128, MODE>(x, n, z, start, 0, seg_rows, ws, ws_bytes, st, SegArgs(), start_dev);
       default: return TCU_ERR_ARG;
     }
   }
@@ -358,6 +359,15 @@ tcu_status_t tcu_selftest_wait_timeout(int which, uint64_t timeout_ns, void* ws,
                                                            timeout_ns);
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? TCU_OK : cuda_fail(e, "selftest_wait_kernel launch");
+}
+
+tcu_status_t tcu_scan_chained(const void* x, tcu_dtype_t x_dtype, int64_t n, int S, double start,
+                              const void* start_dev, void* z, void* ws, size_t ws_bytes, void* stream) {
+  if (n < 0) return TCU_ERR_ARG;
+  if (n == 0) return TCU_OK;
+  if (!x || !z) return TCU_ERR_ARG;
+  if (!aligned16(x) || !aligned16(z) || (reinterpret_cast<uintptr_t>(start_dev) & 3u)) return TCU_ERR_ALIGN;
+  return dispatch_scan<kScanFull>(x, x_dtype, n, S, z, start, 0, ws, ws_bytes, (cudaStream_t)stream, start_dev);
 }
 
 tcu_status_t tcu_scan(const void* x, tcu_dtype_t x_dtype, int64_t n, int S, double start, void* z, void* ws,

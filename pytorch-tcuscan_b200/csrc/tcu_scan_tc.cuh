@@ -61,6 +61,7 @@ struct ScanParams {
   int64_t num_tiles;
   double start_f;     // starting value (run_scan_single_core's starting_sum)
   long long start_i;
+  const void* start_dev;  // optional: one output element (int32 / fp32) added to the start (chained chunks)
   WsHeader* ws;
   TileDesc* descs;
   uint64_t timeout_ns;
@@ -192,6 +193,15 @@ __device__ __forceinline__ float load_at(const void* x, int64_t e) {
   } else {
     return load_elem<InT>(static_cast<const InT*>(x) + e);
   }
+}
+
+// Starting value of a full scan: the host-given start plus, for chained
+// chunks, the previous chunk's last output read from device memory.
+template <typename V, bool IS_INT, typename P>
+__device__ __forceinline__ V scan_start(const P& p) {
+  V s = IS_INT ? (V)p.start_i : (V)p.start_f;
+  if (p.start_dev) s += IS_INT ? (V)*static_cast<const int*>(p.start_dev) : (V)*static_cast<const float*>(p.start_dev);
+  return s;
 }
 
 // Segmented carry operator on (flag, value): (f1,v1) + (f2,v2) =
@@ -347,7 +357,7 @@ __device__ __forceinline__ void scan_epilogue(const ScanParams& p, const CUtenso
   const int wg_thread = threadIdx.x - 64 - g * 128;
   const uint32_t bar_id = 1 + g;
   uint8_t* stg_base = smem + C::OFF_STG + g * C::STG_BUFS * C::STG_BYTES;
-  const V start = IS_INT ? (V)p.start_i : (V)p.start_f;
+  const V start = scan_start<V, IS_INT>(p);
   uint32_t nfill = 0;
 
   const bool prof = p.phase_ns != nullptr && wg_thread == 0;
@@ -641,7 +651,7 @@ __device__ __forceinline__ void scan_summer(const ScanParams& p, uint8_t* smem, 
   constexpr int BPT = C::BPT;
   using V = typename std::conditional<IS_INT, long long, double>::type;
   const int lane = threadIdx.x & 31;
-  const V start = IS_INT ? (V)p.start_i : (V)p.start_f;
+  const V start = scan_start<V, IS_INT>(p);
   const bool prof = p.phase_ns != nullptr && lane == 0;
   // Modes whose tile aggregate this warp publishes as soon as the data lands:
   // the full scan, and the segmented modes whose last segment start in a tile
