@@ -50,7 +50,8 @@ typedef enum tcu_dtype {
   TCU_BFLOAT16 = 6,
   TCU_FLOAT32 = 7,
   TCU_FLOAT64 = 8,
-  TCU_UINT32 = 9
+  TCU_UINT32 = 9,
+  TCU_UINT8 = 10
 } tcu_dtype_t;
 
 /* ---- library / workspace ------------------------------------------------ */
@@ -212,6 +213,16 @@ TCU_API tcu_status_t tcu_compress_counted(const void* x, int elem_bytes, const i
 TCU_API tcu_status_t tcu_compress_segments(const void* x, int elem_bytes, const int8_t* mask, int64_t n,
                                            const int64_t* seg_starts, int64_t nseg, void* out, int64_t capacity,
                                            int64_t* seg_pos, void* ws, size_t ws_bytes, void* stream);
+/* Stable partition: out[0, k) = x[mask != 0] and out[k, n) = x[mask == 0],
+ * both in input order (k = number selected, written to count_dev as int64
+ * when given).  idx_mode 0: values only; 1: idx_in (idx_bytes 4 or 8)
+ * permuted the same way into idx_out.  out / idx_out hold n elements.  Same
+ * passes and workspace as tcu_compress.  Replaces run_split
+ * (src/torch/torch_split.h:33-79) and run_split_ind (:91-142), which take
+ * 16-bit elements only; any of 1, 2, 4 or 8 bytes here.                   */
+TCU_API tcu_status_t tcu_split(const void* x, int elem_bytes, const int8_t* mask, int64_t n, const void* idx_in,
+                               int idx_bytes, int idx_mode, void* out, void* idx_out, void* count_dev, void* ws,
+                               size_t ws_bytes, void* stream);
 /* Number of mask != 0 into a device uint64 (the reference sizes compress
  * outputs with run_reduce_tiles + .sum(), src/torch/torch_compress.h:62-64). */
 TCU_API tcu_status_t tcu_mask_count(const int8_t* mask, int64_t n, void* count_dev, void* stream);
@@ -230,6 +241,40 @@ TCU_API tcu_status_t tcu_csr_gather(const void* values, tcu_dtype_t dtype, const
  * reference's v1 SpMV.                                                     */
 TCU_API tcu_status_t tcu_gather_spmv(const void* values, int elem_bytes, int64_t n_values, const void* idxs,
                                      tcu_dtype_t idx_dtype, int64_t n_idx, void* z, void* ws, void* stream);
+
+/* ---- radix sort and top-k ------------------------------------------------
+ * Ascending stable sort with int32 positions: out = sorted x, idx_out[i] =
+ * position in x of out[i] (0-based), n <= 2^31 - 1.  Keys of 1, 2 or 4
+ * bytes (int8/uint8, int16/fp16/bf16, int32/uint32/fp32) in byte-digit LSD
+ * passes.  Floats are ordered by the reference's encoding: negatives below
+ * positives, -0 below +0, NaNs with the sign bit first and NaNs without it
+ * last.  tmp: device scratch of tcu_radix_sort_tmp_bytes(dtype, n) bytes,
+ * 256-byte aligned, no initialisation needed.  Replaces run_radix_sort
+ * (src/torch/torch_sort.h:30-82; fp16 / int16 there).                     */
+TCU_API size_t tcu_radix_sort_tmp_bytes(tcu_dtype_t dtype, int64_t n);
+TCU_API tcu_status_t tcu_radix_sort(const void* x, tcu_dtype_t dtype, int64_t n, void* out, int32_t* idx_out,
+                                    void* tmp, size_t tmp_bytes, void* stream);
+/* The k largest elements of x (int16, fp16 or bf16) and their int32
+ * positions, in input order: every element above the k-th largest value
+ * and, of the elements equal to it, the lowest-positioned ones.  NaN ranks
+ * above every number and -0 equals +0 (value comparisons, as the reference's
+ * x <= pivot splits).  0 <= k <= n.  tmp: tcu_topk_tmp_bytes(n) bytes,
+ * 256-byte aligned.  Replaces run_topk_int16 / run_topk_fp16
+ * (src/torch/torch_topk.h:86-211), which return the same set band by band;
+ * their x_min / x_max bisection bounds are not needed here.               */
+TCU_API size_t tcu_topk_tmp_bytes(int64_t n);
+TCU_API tcu_status_t tcu_topk(const void* x, tcu_dtype_t dtype, int64_t n, int64_t k, void* out, int32_t* idx_out,
+                              void* tmp, size_t tmp_bytes, void* stream);
+/* Lower-bound estimates of the k-th largest value, one per block (fp16):
+ * tcu_topk_pivot_blocks(n, num_samples) blocks = min(SM count, tiles of
+ * num_samples * 32 elements); block b samples 8 tiles from tile
+ * b * ceil(tiles / blocks); per tile the k_outer-th largest of the groups'
+ * k_inner-th largest values (32-element groups).  Replaces
+ * run_topk_pivot_fp16 (src/torch/torch_topk.h:35-73, k_inner 8 and
+ * k_outer 4 there).                                                        */
+TCU_API int tcu_topk_pivot_blocks(int64_t n, int num_samples);
+TCU_API tcu_status_t tcu_topk_pivot(const void* x, tcu_dtype_t dtype, int64_t n, int num_samples, int k_inner,
+                                    int k_outer, void* out, void* stream);
 
 /* ---- scan phases as standalone operators ----------------------------------
  * reduce_tiles: z[b] = sum of block b, block = tile_len * ceil(ceil(n /

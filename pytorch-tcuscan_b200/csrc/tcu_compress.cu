@@ -157,8 +157,11 @@ __device__ __forceinline__ void vec_set(uint4* v, int j, typename ElemT<EB>::T e
 }
 
 // IDX: 0 none, 1 gather idx_in (IB bytes), 2 positions (int32 when IB == 4,
-// int64 when IB == 8).
-template <int EB, int IDX, int IB>
+// int64 when IB == 8).  SPLIT: stable partition instead of compaction -- every
+// element is written, the selected ones at their compaction offsets and the
+// others after all selected ones (at total + the unselected elements before
+// them), so a tile writes two runs.
+template <int EB, int IDX, int IB, bool SPLIT>
 __global__ void __launch_bounds__(kCmpThreads, 1)
     compress_kernel(const __grid_constant__ CUtensorMap mmap, const __grid_constant__ CUtensorMap xmap,
                     const __grid_constant__ CUtensorMap imap, const CompressParams p) {
@@ -257,7 +260,7 @@ __global__ void __launch_bounds__(kCmpThreads, 1)
           const uint4 m = *reinterpret_cast<const uint4*>(st + row_chunk(wg_thread, v, C::SPAN_M));
           sel |= (unsigned long long)(sel4(m.x) | (sel4(m.y) << 4) | (sel4(m.z) << 8) | (sel4(m.w) << 12)) << (16 * v);
         }
-        if (sel) {
+        if (SPLIT || sel) {
 #pragma unroll
           for (int v = 0; v < C::SPAN_X / 16; ++v)
             xr[v] = *reinterpret_cast<const uint4*>(st + C::X_OFF + row_chunk(wg_thread, v, C::SPAN_X));
@@ -274,10 +277,13 @@ __global__ void __launch_bounds__(kCmpThreads, 1)
         for (int v = 0; v < (IDX == 1 ? C::SPAN_I / 16 : 1); ++v) ir[v] = make_uint4(0, 0, 0, 0);
 #pragma unroll
         for (int j = 0; j < EPT; ++j) {
-          if (e0 + j < p.n && p.mask[e0 + j] != 0) {
-            sel |= 1ull << j;
-            vec_set<EB>(xr, j, static_cast<const T*>(p.x)[e0 + j]);
-            if constexpr (IDX == 1) vec_set<(IB > 0 ? IB : 4)>(ir, j, static_cast<const I*>(p.idx_in)[e0 + j]);
+          if (e0 + j < p.n) {
+            const bool on = p.mask[e0 + j] != 0;
+            if (on) sel |= 1ull << j;
+            if (SPLIT || on) {
+              vec_set<EB>(xr, j, static_cast<const T*>(p.x)[e0 + j]);
+              if constexpr (IDX == 1) vec_set<(IB > 0 ? IB : 4)>(ir, j, static_cast<const I*>(p.idx_in)[e0 + j]);
+            }
           }
         }
       }
@@ -306,13 +312,31 @@ __global__ void __launch_bounds__(kCmpThreads, 1)
         T* sx = reinterpret_cast<T*>(st + C::X_OFF);
         I* si = reinterpret_cast<I*>(st + C::I_OFF);
         int o = local;
+        if constexpr (SPLIT) {
+          // unselected elements before this row: all earlier rows of the tile are full
+          int u = total + wg_thread * EPT - local;
+          const int nv = in_smem ? EPT : (is_tail ? (int)(p.n - e0) : 0);
 #pragma unroll
-        for (int j = 0; j < EPT; ++j) {
-          if ((sel >> j) & 1ull) {
-            sx[o] = vec_elem<EB>(xr, j);
-            if constexpr (IDX == 1) si[o] = (I)vec_elem<(IB > 0 ? IB : 4)>(ir, j);
-            if constexpr (IDX == 2) si[o] = (I)(e0 + j);
-            ++o;
+          for (int j = 0; j < EPT; ++j) {
+            if (j < nv) {
+              const bool on = (sel >> j) & 1ull;
+              const int d = on ? o : u;
+              sx[d] = vec_elem<EB>(xr, j);
+              if constexpr (IDX == 1) si[d] = (I)vec_elem<(IB > 0 ? IB : 4)>(ir, j);
+              if constexpr (IDX == 2) si[d] = (I)(e0 + j);
+              o += on ? 1 : 0;
+              u += on ? 0 : 1;
+            }
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < EPT; ++j) {
+            if ((sel >> j) & 1ull) {
+              sx[o] = vec_elem<EB>(xr, j);
+              if constexpr (IDX == 1) si[o] = (I)vec_elem<(IB > 0 ? IB : 4)>(ir, j);
+              if constexpr (IDX == 2) si[o] = (I)(e0 + j);
+              ++o;
+            }
           }
         }
       }
@@ -322,8 +346,12 @@ __global__ void __launch_bounds__(kCmpThreads, 1)
       {
         const T* sx = reinterpret_cast<const T*>(st + C::X_OFF);
         const I* si = reinterpret_cast<const I*>(st + C::I_OFF);
-        for (int i = wg_thread; i < total; i += 128) {
-          const long long g = pre + i;
+        const int64_t t0 = (int64_t)tid * TILE;
+        const int valid = SPLIT ? (int)(p.n - t0 < TILE ? p.n - t0 : TILE) : total;
+        // selected run at pre, unselected run after every selected element
+        const long long ubase = SPLIT ? p.offsets[p.num_tiles] + (t0 - pre) - total : 0;
+        for (int i = wg_thread; i < valid; i += 128) {
+          const long long g = i < total ? pre + i : ubase + i;
           if (g < p.capacity) {
             static_cast<T*>(p.out)[g] = sx[i];
             if constexpr (IDX != 0) static_cast<I*>(p.idx_out)[g] = si[i];
@@ -509,7 +537,7 @@ static tcu_status_t cmp_count(const int8_t* mask, int64_t n, int64_t tile, const
   return e == cudaSuccess ? TCU_OK : cuda_fail(e, "compress count launch");
 }
 
-template <int EB, int IDX, int IB>
+template <int EB, int IDX, int IB, bool SPLIT>
 static tcu_status_t launch_compress(CompressParams& p, cudaStream_t st) {
   using C = CmpCfg<EB, IDX, IB>;
   p.full_rows = p.n / C::EPT;
@@ -525,7 +553,7 @@ static tcu_status_t launch_compress(CompressParams& p, cudaStream_t st) {
       s = make_map_2d(&im, p.idx_in, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, C::SPAN_I, p.full_rows, C::SPAN_I, 128);
     if (s != TCU_OK) return s;
   }
-  auto kern = compress_kernel<EB, IDX, IB>;
+  auto kern = compress_kernel<EB, IDX, IB, SPLIT>;
   static bool attr_set = false;
   if (!attr_set) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM);
@@ -553,7 +581,7 @@ static tcu_status_t cmp_check(const void* x, int elem_bytes, const int8_t* mask,
 // The compaction pass, with the tile offsets already in the workspace.
 static tcu_status_t cmp_run(const void* x, int elem_bytes, const int8_t* mask, int64_t n, const void* idx_in,
                             int idx_bytes, int idx_mode, void* out, void* idx_out, int64_t capacity,
-                            const CmpScratch& sc, void* ws, cudaStream_t st) {
+                            const CmpScratch& sc, void* ws, cudaStream_t st, bool split = false) {
   CompressParams p{};
   p.x = x;
   p.mask = mask;
@@ -565,7 +593,21 @@ static tcu_status_t cmp_run(const void* x, int elem_bytes, const int8_t* mask, i
   p.offsets = sc.offsets;
   p.ws = static_cast<WsHeader*>(ws);
   p.timeout_ns = timeout_ns();
-#define TCU_CMP(EB, IDX, IB) return launch_compress<EB, IDX, IB>(p, st)
+  if (split) {  // stable partition: values only or with gathered indices
+#define TCU_SPL(EB)                                                        \
+  if (idx_mode == 0) return launch_compress<EB, 0, 0, true>(p, st);       \
+  if (idx_bytes == 4) return launch_compress<EB, 1, 4, true>(p, st);      \
+  return launch_compress<EB, 1, 8, true>(p, st)
+    if (idx_mode == 2) return TCU_ERR_ARG;
+    switch (elem_bytes) {
+      case 1: TCU_SPL(1);
+      case 2: TCU_SPL(2);
+      case 4: TCU_SPL(4);
+      default: TCU_SPL(8);
+    }
+#undef TCU_SPL
+  }
+#define TCU_CMP(EB, IDX, IB) return launch_compress<EB, IDX, IB, false>(p, st)
   switch (elem_bytes) {
     case 1:
       if (idx_mode == 0) TCU_CMP(1, 0, 0);
@@ -696,6 +738,30 @@ tcu_status_t tcu_compress_segments(const void* x, int elem_bytes, const int8_t* 
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "seg_positions_kernel launch");
   }
+  return cmp_clear(ws, sc, st);
+}
+
+// Stable partition (the reference's run_split / run_split_ind,
+// src/torch/torch_split.h:33-79 and :91-142): out[0, k) = x[mask != 0],
+// out[k, n) = x[mask == 0], both in input order; with idx_mode 1 the same
+// permutation is applied to idx_in.  One count pass, one offset scan, one
+// streaming pass that writes both runs of every tile.
+tcu_status_t tcu_split(const void* x, int elem_bytes, const int8_t* mask, int64_t n, const void* idx_in, int idx_bytes,
+                       int idx_mode, void* out, void* idx_out, void* count_dev, void* ws, size_t ws_bytes,
+                       void* stream) {
+  if (n < 0) return TCU_ERR_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (n == 0) return zero_count(count_dev, st);
+  if (idx_mode != 0 && idx_mode != 1) return TCU_ERR_ARG;
+  tcu_status_t s = cmp_check(x, elem_bytes, mask, idx_in, idx_bytes, idx_mode, out, idx_out);
+  if (s != TCU_OK) return s;
+  if (reinterpret_cast<uintptr_t>(count_dev) & 7u) return TCU_ERR_ALIGN;
+  const int64_t tile = compress_tile(elem_bytes, idx_stage_bytes(idx_mode, idx_bytes));
+  CmpScratch sc;
+  s = cmp_scratch(ws, ws_bytes, n, tile, &sc);
+  if (s == TCU_OK) s = cmp_count(mask, n, tile, sc, static_cast<long long*>(count_dev), st);
+  if (s == TCU_OK) s = cmp_run(x, elem_bytes, mask, n, idx_in, idx_bytes, idx_mode, out, idx_out, n, sc, ws, st, true);
+  if (s != TCU_OK) return s;
   return cmp_clear(ws, sc, st);
 }
 

@@ -304,6 +304,144 @@ def run_where(x, pivot, S):
 
 
 # ---------------------------------------------------------------------------
+# split, radix sort, top-k (src/torch/torch_split.h, torch_sort.h, torch_topk.h)
+
+def _split(x, mask, indices_in, where):
+    n = x.numel()
+    z = torch.empty_like(x)
+    idx_out = torch.empty_like(indices_in) if indices_in is not None else None
+    if n == 0:
+        return z, idx_out
+    from tcuscan_b200 import autotune
+
+    autotune.apply_ctas(autotune.best("compress", x.dtype, n)[1])
+    ib = indices_in.element_size() if indices_in is not None else 0
+    ws, wsb = workspace(x.device, _lib.lib.tcu_workspace_bytes(n, 64))
+    check(_lib.lib.tcu_split(x.data_ptr(), x.element_size(), mask.data_ptr(), n,
+                             indices_in.data_ptr() if indices_in is not None else None, ib,
+                             1 if indices_in is not None else 0, z.data_ptr(),
+                             idx_out.data_ptr() if idx_out is not None else None, None, ws, wsb,
+                             stream_ptr(x.device)), where)
+    _after(x)
+    return z, idx_out
+
+
+def run_split(x, mask, S):
+    """Stable partition: x[mask != 0] followed by x[mask == 0], n elements
+    (reference: src/torch/torch_split.h:33-79, 16-bit dtypes only there; any
+    1/2/4/8-byte dtype here).  One count pass, one offset scan, one streaming
+    pass writing both runs; asynchronous (the reference synchronises)."""
+    _check_S_opt(S)
+    x = _cuda_input(x)
+    mask = _mask_input(mask, x.numel(), x.device)
+    return _split(x, mask, None, "run_split")[0]
+
+
+def run_split_ind(x, mask, indices_in, S):
+    """(split of x, indices_in permuted the same way) (reference:
+    src/torch/torch_split.h:91-142; indices int32 there, int32 or int64
+    here)."""
+    _check_S_opt(S)
+    x = _cuda_input(x)
+    mask = _mask_input(mask, x.numel(), x.device)
+    indices_in = _cuda_input(indices_in, "indices_in")
+    if indices_in.numel() != x.numel():
+        raise ValueError("indices_in must have the length of x")
+    if indices_in.dtype not in (torch.int32, torch.int64):
+        raise TypeError(f"indices_in must be int32 or int64, got {indices_in.dtype}")
+    return _split(x, mask, indices_in, "run_split_ind")
+
+
+_SORT_DTYPES = (torch.int8, torch.uint8, torch.int16, torch.float16, torch.bfloat16, torch.int32, torch.float32)
+
+
+def run_radix_sort(x, S):
+    """(ascending stable sort of x, int32 positions) (reference:
+    src/torch/torch_sort.h:30-82; fp16 / int16 and lengths that are multiples
+    of the tile there).  Byte-digit LSD passes: two for 16-bit keys.  Floats
+    follow the reference's bit encoding: -0 sorts below +0, NaNs with the
+    sign bit first and the others last."""
+    _check_S_opt(S)
+    x = _cuda_input(x)
+    if x.dtype not in _SORT_DTYPES:
+        raise TypeError(f"run_radix_sort: unsupported dtype {x.dtype}")
+    n = x.numel()
+    if n > 0x7FFFFFFF:
+        raise ValueError("run_radix_sort: more than 2^31 - 1 elements (int32 positions)")
+    out = torch.empty_like(x)
+    idx = torch.empty(n, dtype=torch.int32, device=x.device)
+    if n == 0:
+        return out, idx
+    code = _lib.DTYPE_CODE[x.dtype]
+    tb = _lib.lib.tcu_radix_sort_tmp_bytes(code, n)
+    tmp = torch.empty(tb, dtype=torch.uint8, device=x.device)
+    check(_lib.lib.tcu_radix_sort(x.data_ptr(), code, n, out.data_ptr(), idx.data_ptr(), tmp.data_ptr(), tb,
+                                  stream_ptr(x.device)), "run_radix_sort")
+    _after(x)
+    return out, idx
+
+
+def _topk(x, k, dtype, where):
+    x = _cuda_input(x)
+    if x.dtype != dtype:
+        raise TypeError(f"{where}: x must be {dtype}, got {x.dtype}")
+    n = x.numel()
+    k = int(k)
+    if k < 0 or k > n:
+        raise ValueError(f"{where}: k = {k} outside [0, {n}]")
+    if n > 0x7FFFFFFF:
+        raise ValueError(f"{where}: more than 2^31 - 1 elements (int32 positions)")
+    out = torch.empty(k, dtype=x.dtype, device=x.device)
+    idx = torch.empty(k, dtype=torch.int32, device=x.device)
+    if k == 0:
+        return out, idx
+    tb = _lib.lib.tcu_topk_tmp_bytes(n)
+    tmp = torch.empty(tb, dtype=torch.uint8, device=x.device)
+    check(_lib.lib.tcu_topk(x.data_ptr(), _lib.DTYPE_CODE[x.dtype], n, k, out.data_ptr(), idx.data_ptr(),
+                            tmp.data_ptr(), tb, stream_ptr(x.device)), where)
+    _after(x)
+    return out, idx
+
+
+def run_topk_int16(x, k, x_min, x_max, S):
+    """(k largest of x, int32 positions), in input order (reference:
+    src/torch/torch_topk.h:86-145, which bisects [x_min, x_max] with repeated
+    splits and returns the same set band by band).  Ties at the k-th value
+    keep the lowest positions, as the reference's stable splits do.  x_min and
+    x_max are accepted for the signature; the radix select does not need
+    them."""
+    _check_S_opt(S)
+    return _topk(x, k, torch.int16, "run_topk_int16")
+
+
+def run_topk_fp16(x, k, x_min, x_max, S):
+    """fp16 form of run_topk_int16 (reference: src/torch/torch_topk.h:157-211).
+    NaN ranks above every number; -0 and +0 are equal."""
+    _check_S_opt(S)
+    return _topk(x, k, torch.float16, "run_topk_fp16")
+
+
+def run_topk_pivot_fp16(x, k, num_samples=32):
+    """Per-block lower-bound estimates of the k-th largest value (reference:
+    src/torch/torch_topk.h:35-73; k is ignored there too, k_inner = 8,
+    k_outer = 4).  One estimate per block, min(SM count, tiles of
+    num_samples * 32 elements) blocks."""
+    x = _cuda_input(x)
+    if x.dtype != torch.float16:
+        raise TypeError(f"run_topk_pivot_fp16: x must be float16, got {x.dtype}")
+    n = x.numel()
+    num_samples = int(num_samples)
+    if n == 0 or num_samples <= 0:
+        raise ValueError("run_topk_pivot_fp16: empty input or num_samples <= 0")
+    b = _lib.lib.tcu_topk_pivot_blocks(n, num_samples)
+    out = torch.empty(b, dtype=torch.float16, device=x.device)
+    check(_lib.lib.tcu_topk_pivot(x.data_ptr(), _lib.DTYPE_CODE[x.dtype], n, num_samples, 8, 4, out.data_ptr(),
+                                  stream_ptr(x.device)), "run_topk_pivot_fp16")
+    _after(x)
+    return out
+
+
+# ---------------------------------------------------------------------------
 # gather (src/torch/torch_gather.h)
 
 def run_csr_gather(values, cols, x):

@@ -27,6 +27,7 @@ TCU_ERR_OOM, TCU_ERR_ALIGN, TCU_ERR_DEVICE, TCU_ERR_WORKSPACE = 5, 6, 7, 8
 # dtype codes
 TCU_INT8, TCU_INT16, TCU_INT32, TCU_INT64 = 1, 2, 3, 4
 TCU_FLOAT16, TCU_BFLOAT16, TCU_FLOAT32, TCU_FLOAT64, TCU_UINT32 = 5, 6, 7, 8, 9
+TCU_UINT8 = 10
 
 DTYPE_CODE = {
     torch.int8: TCU_INT8,
@@ -37,6 +38,7 @@ DTYPE_CODE = {
     torch.bfloat16: TCU_BFLOAT16,
     torch.float32: TCU_FLOAT32,
     torch.float64: TCU_FLOAT64,
+    torch.uint8: TCU_UINT8,
 }
 if hasattr(torch, "uint32"):
     DTYPE_CODE[torch.uint32] = TCU_UINT32
@@ -79,6 +81,13 @@ _sig("tcu_mask_count", _ST, _P, _I64, _P, _P)
 _sig("tcu_compress_count", _ST, _P, _I64, _I, _I, _I, _P, _P, _SZ, _P)
 _sig("tcu_compress_counted", _ST, _P, _I, _P, _I64, _P, _I, _I, _P, _P, _I64, _P, _SZ, _P)
 _sig("tcu_compress_segments", _ST, _P, _I, _P, _I64, _P, _I64, _P, _I64, _P, _P, _SZ, _P)
+_sig("tcu_split", _ST, _P, _I, _P, _I64, _P, _I, _I, _P, _P, _P, _P, _SZ, _P)
+_sig("tcu_radix_sort_tmp_bytes", _SZ, _I, _I64)
+_sig("tcu_radix_sort", _ST, _P, _I, _I64, _P, _P, _P, _SZ, _P)
+_sig("tcu_topk_tmp_bytes", _SZ, _I64)
+_sig("tcu_topk", _ST, _P, _I, _I64, _I64, _P, _P, _P, _SZ, _P)
+_sig("tcu_topk_pivot_blocks", _I, _I64, _I)
+_sig("tcu_topk_pivot", _ST, _P, _I, _I64, _I, _I, _I, _P, _P)
 _sig("tcu_pack", _ST, _P, _I64, _I, _I, _P, _I64, _P)
 _sig("tcu_csr_gather", _ST, _P, _I, _P, _I64, _P, _I64, _P, _P, _P)
 _sig("tcu_gather_spmv", _ST, _P, _I, _I64, _P, _I, _I64, _P, _P, _P)
