@@ -195,7 +195,26 @@ def measure_extras(dev, steps=10, warmup=3):
     ar = torch.arange(n, dtype=torch.int32, device=dev)
     ms = _device_ms(lambda: tcuscan_ops.run_compress_ind(xv, ar, mask, 64), 3, 1)
     out["compress_ind_f16_arange_incl_count_sync"] = entry(n, n * 7 + k * 6, ms, selected=k)
+    # split (stable partition) of the same values: reads x and the mask, writes n
+    ms = _device_ms(lambda: tcuscan_ops.run_split(xv, mask, 64), steps, warmup)
+    out["split_f16_2e28"] = entry(n, n * 5, ms, selected=k)
     del xv, mask, ar
+
+    # radix sort (values + int32 positions): the reference's largest sort size
+    # and 2^28; algorithmic bytes = read 2 B, write 2 + 4 B per element
+    for name, ns in (("radix_sort_f16_25165824", 25165824), ("radix_sort_f16_2e28", n)):
+        xs = torch.rand(ns, device=dev).half()
+        ms = _device_ms(lambda: tcuscan_ops.run_radix_sort(xs, 128), steps, warmup)
+        out[name] = entry(ns, ns * 8, ms)
+        del xs
+    # top-k, fp16 U[0,1), n = 20 Mi - 10, k = sqrt(n) (the reference's largest
+    # top-k test); algorithmic bytes = one read of x
+    nt = 20 * 1024 * 1024 - 10
+    xt = torch.rand(nt, device=dev).half()
+    kt = int(nt ** 0.5)
+    ms = _device_ms(lambda: tcuscan_ops.run_topk_fp16(xt, kt, 0.0, 1.0, 128), steps, warmup)
+    out["topk_f16_20Mi_ksqrt"] = entry(nt, nt * 2, ms, k=kt)
+    del xt
 
     # flag-driven segmented scan (starts), fp16 2^28, flags Bernoulli(0.01)
     xf = workloads.scan_input(n, torch.float16, dev, seed=12)
@@ -540,7 +559,7 @@ def run_reference_arm(args):
 
 
 PROFILE_OPS = ("compress_f16", "compress_f32", "compress_ind_f16", "spmv_f32", "spmv_f16", "serve", "segscan_i8",
-               "segscan_f16", "segsum_i8", "segsum_f16", "segsum_f32")
+               "segscan_f16", "segsum_i8", "segsum_f16", "segsum_f32", "split_f16", "sort_f16", "topk_f16")
 
 
 def run_profile_op(args, dev):
@@ -568,6 +587,20 @@ def run_profile_op(args, dev):
             fn = lambda: tcuscan_ops.run_compress_pos(xv, mask, k, 64)  # noqa: E731
             nbytes = n * (eb + 1) + k * eb
         units = n
+    elif op in ("split_f16", "sort_f16", "topk_f16"):
+        xv = torch.rand(n, device=dev).half()
+        units = n
+        if op == "split_f16":
+            mask = workloads.bernoulli_mask(n, 0.3, dev, seed=8)
+            fn = lambda: tcuscan_ops.run_split(xv, mask, 64)  # noqa: E731
+            nbytes = n * 5
+        elif op == "sort_f16":
+            fn = lambda: tcuscan_ops.run_radix_sort(xv, 128)  # noqa: E731
+            nbytes = n * 8
+        else:
+            kt = int(n ** 0.5)
+            fn = lambda: tcuscan_ops.run_topk_fp16(xv, kt, 0.0, 1.0, 128)  # noqa: E731
+            nbytes = n * 2
     elif op.startswith("spmv"):
         dt = torch.float32 if op == "spmv_f32" else torch.float16
         vals, indptr, cols, xs = workloads.zipf_csr(target_nnz=min(n, 1 << 26), dtype=dt, device=dev, seed=9)

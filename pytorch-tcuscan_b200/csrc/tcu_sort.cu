@@ -9,13 +9,14 @@
 // largest value from sampled 32-element groups.
 //
 // Here the same results come from byte-digit passes bound by HBM:
-//   radix sort   8-bit LSD passes (2 for 16-bit keys).  Each pass: per-tile
-//                digit counts (rs_hist_kernel), one exclusive scan per digit
-//                over the tiles (rs_offsets_kernel), and a scatter pass
-//                (rs_scatter_kernel) that ranks the tile's keys stably per
-//                digit with warp match votes, sorts the tile by digit in
-//                shared memory and writes each digit's run to its global
-//                offset, so stores are runs of consecutive addresses.
+//   radix sort   8-bit LSD passes (2 for 16-bit keys).  Each pass: digit
+//                counts per chunk of tiles (rs_hist_kernel, one CTA per
+//                chunk), one scan of the chunk counts (rs_chunk_scan_kernel),
+//                and a scatter pass over the same chunks (rs_scatter_kernel)
+//                that ranks each tile's keys stably per digit with warp
+//                ballots, sorts the tile by digit in shared memory and writes
+//                each digit's run at the chunk's running position, so stores
+//                are runs of consecutive addresses.
 //   top-k        a radix select: 256-bin histograms of the key's high byte,
 //                then of the low byte inside the chosen high byte, fix the
 //                k-th largest key t; a count pass, one offset scan and an
@@ -89,90 +90,173 @@ __device__ __forceinline__ int block_excl_scan256(int v, int* sw, int* total) {
 }
 
 // ---------------------------------------------------------------------------
-// Radix sort.
-//
-// Per-tile digit counts, counts[tile * 256 + digit], and the digit totals of
-// the whole input (totals must be zero on entry).  FIRST: keys are the raw
-// input bits and are encoded on the fly.
-template <typename K, int CODEC, bool FIRST>
-__global__ void __launch_bounds__(kRsThreads) rs_hist_kernel(const K* __restrict__ keys, int64_t n, int shift,
-                                                             int64_t num_tiles, int* __restrict__ counts,
-                                                             unsigned* __restrict__ totals) {
-  __shared__ int s_h[kRsWarps][kRsDigits];
-  __shared__ unsigned s_tot[kRsDigits];
-  const int w = threadIdx.x >> 5;
-  s_tot[threadIdx.x] = 0;
-  for (int64_t t = blockIdx.x; t < num_tiles; t += gridDim.x) {
+// Radix sort.  The tiles are split into contiguous chunks, one per CTA, the
+// same for the counting and the scatter kernel of a pass, so a CTA carries
+// its running per-digit output positions from tile to tile and no per-tile
+// offsets are stored.
+
+// Lanes of the warp whose digit equals this lane's (eight ballots).
+__device__ __forceinline__ unsigned digit_peers(int d) {
+  unsigned p = 0xffffffffu;
 #pragma unroll
-    for (int k = 0; k < kRsWarps; ++k) s_h[k][threadIdx.x] = 0;
-    __syncthreads();
-    const int64_t t0 = t * kRsTile;
+  for (int b = 0; b < 8; ++b) {
+    const bool on = (d >> b) & 1;
+    const unsigned bb = __ballot_sync(0xffffffffu, on);
+    p &= on ? bb : ~bb;
+  }
+  return p;
+}
+
+__host__ __device__ inline int64_t chunk_tiles(int64_t num_tiles, int chunks) {
+  return (num_tiles + chunks - 1) / chunks;
+}
+
+// 256-bin histograms in shared memory: four counter copies per warp
+// (lane % 4), so equal digits in one warp spread over four addresses.
+constexpr int kHistCopies = kRsWarps * 4;
+
+__device__ __forceinline__ int* hist_slot(int* s_h) {
+  return s_h + (((threadIdx.x >> 5) << 2) + (threadIdx.x & 3)) * kRsDigits;
+}
+
+// Counts digit(key) >= 0 of keys[lo, hi) into s_h (kHistCopies x 256 ints):
+// per round every thread has four 16-byte loads in flight (VEC: keys 16-byte
+// aligned; lo a multiple of the vector length).  Called by all threads.
+template <typename K, bool VEC, typename DigitF>
+__device__ __forceinline__ void smem_hist_range(const K* __restrict__ keys, int64_t lo, int64_t hi, int* s_h,
+                                                DigitF digit) {
+  constexpr int KPV = 16 / (int)sizeof(K);
+  constexpr int VPT = 4;
+  constexpr int PER = KPV * VPT;
+  int* slot = hist_slot(s_h);
+  for (int64_t b = lo; b < hi; b += (int64_t)kRsThreads * PER) {  // block-uniform
+    union {
+      uint4 u[VPT];
+      K k[PER];
+    } kv;
 #pragma unroll
-    for (int j = 0; j < kRsEpt; ++j) {
-      const int64_t e = t0 + j * kRsThreads + threadIdx.x;
-      if (e < n) {
-        K k = keys[e];
-        if constexpr (FIRST) k = key_enc<K, CODEC>(k);
-        atomicAdd(&s_h[w][(k >> shift) & 0xFF], 1);
+    for (int v = 0; v < VPT; ++v) {
+      const int64_t e = b + ((int64_t)v * kRsThreads + threadIdx.x) * KPV;
+      if (VEC && e + KPV <= hi) {
+        kv.u[v] = __ldg(reinterpret_cast<const uint4*>(keys + e));
+      } else {
+#pragma unroll
+        for (int i = 0; i < KPV; ++i) kv.k[v * KPV + i] = e + i < hi ? keys[e + i] : (K)0;
       }
     }
-    __syncthreads();
-    int c = 0;
 #pragma unroll
-    for (int k = 0; k < kRsWarps; ++k) c += s_h[k][threadIdx.x];
-    counts[t * kRsDigits + threadIdx.x] = c;
-    s_tot[threadIdx.x] += (unsigned)c;
-    __syncthreads();
+    for (int v = 0; v < VPT; ++v) {
+      const int64_t e = b + ((int64_t)v * kRsThreads + threadIdx.x) * KPV;
+#pragma unroll
+      for (int i = 0; i < KPV; ++i) {
+        const int d = digit(kv.k[v * KPV + i]);
+        if (e + i < hi && d >= 0) atomicAdd(slot + d, 1);
+      }
+    }
   }
-  if (s_tot[threadIdx.x]) atomicAdd(&totals[threadIdx.x], s_tot[threadIdx.x]);
 }
 
-// One CTA per digit d: offs[t * 256 + d] = (keys with a smaller digit) +
-// (keys with digit d in tiles before t).
-__global__ void __launch_bounds__(kRsThreads) rs_offsets_kernel(const int* __restrict__ counts,
-                                                                const unsigned* __restrict__ totals, int64_t num_tiles,
-                                                                int* __restrict__ offs) {
+// Thread d: the total of digit d over the copies (after a barrier).
+__device__ __forceinline__ int smem_hist_total(const int* s_h) {
+  int c = 0;
+#pragma unroll
+  for (int k = 0; k < kHistCopies; ++k) c += s_h[k * kRsDigits + threadIdx.x];
+  return c;
+}
+
+template <typename K, int CODEC, bool FIRST>
+struct RsDigit {
+  int shift;
+  __device__ __forceinline__ int operator()(K k) const {
+    if constexpr (FIRST) k = key_enc<K, CODEC>(k);
+    return (int)((k >> shift) & 0xFF);
+  }
+};
+
+// Digit counts of chunk blockIdx.x: sums[c * 256 + digit], and the digit
+// totals (atomically; zero on entry).  FIRST: keys are the raw input bits and
+// are encoded on the fly.
+template <typename K, int CODEC, bool FIRST, bool VEC>
+__global__ void __launch_bounds__(kRsThreads) rs_hist_kernel(const K* __restrict__ keys, int64_t n, int shift,
+                                                             int64_t num_tiles, int* __restrict__ sums,
+                                                             unsigned* __restrict__ totals) {
+  __shared__ int s_h[kHistCopies * kRsDigits];
+#pragma unroll
+  for (int k = 0; k < kHistCopies; ++k) s_h[k * kRsDigits + threadIdx.x] = 0;
+  __syncthreads();
+  const int64_t tpc = chunk_tiles(num_tiles, gridDim.x);
+  const int64_t e_lo = blockIdx.x * tpc * kRsTile;
+  int64_t e_hi = e_lo + tpc * kRsTile;
+  e_hi = e_hi < n ? e_hi : n;
+  smem_hist_range<K, VEC>(keys, e_lo, e_hi, s_h, RsDigit<K, CODEC, FIRST>{shift});
+  __syncthreads();
+  const int c = smem_hist_total(s_h);
+  sums[blockIdx.x * kRsDigits + threadIdx.x] = c;
+  if (c) atomicAdd(&totals[threadIdx.x], (unsigned)c);
+}
+
+// One CTA per digit d: base[c * 256 + d] = (keys with a smaller digit, from
+// the totals) + (keys with digit d in chunks before c).
+constexpr int kChunkScanThreads = 256;
+
+__global__ void __launch_bounds__(kChunkScanThreads) rs_chunk_scan_kernel(const int* __restrict__ sums, int chunks,
+                                                                         const unsigned* __restrict__ totals,
+                                                                         int* __restrict__ base) {
   __shared__ int sw[kRsWarps];
   const int d = blockIdx.x;
-  int below = 0, tot;
-  if (threadIdx.x < d) below = (int)totals[threadIdx.x];
-  block_excl_scan256(below, sw, &tot);
-  const int base = tot;  // sum of the totals of digits < d
-  const int64_t per = (num_tiles + kRsThreads - 1) / kRsThreads;
-  const int64_t b0 = (int64_t)threadIdx.x * per;
-  const int64_t b1 = b0 + per < num_tiles ? b0 + per : num_tiles;
+  int tot;
+  block_excl_scan256(threadIdx.x < d ? (int)totals[threadIdx.x] : 0, sw, &tot);
+  const int below = tot;
+  // chunks c = threadIdx.x * per .. + per - 1 (at most 4 per thread at 3 chunks per SM)
+  const int per = (chunks + kChunkScanThreads - 1) / kChunkScanThreads;
+  const int c0 = threadIdx.x * per;
+  int v[8];
   int sum = 0;
-  for (int64_t t = b0; t < b1; ++t) sum += counts[t * kRsDigits + d];
-  int run = base + block_excl_scan256(sum, sw, &tot);
-  for (int64_t t = b0; t < b1; ++t) {
-    const int c = counts[t * kRsDigits + d];
-    offs[t * kRsDigits + d] = run;
-    run += c;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    v[i] = (i < per && c0 + i < chunks) ? sums[(c0 + i) * kRsDigits + d] : 0;
+    sum += v[i];
+  }
+  for (int c = c0 + 8; c < c0 + per && c < chunks; ++c) sum += sums[c * kRsDigits + d];  // more than 2048 chunks
+  int run = below + block_excl_scan256(sum, sw, &tot);
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    if (i < per && c0 + i < chunks) {
+      base[(c0 + i) * kRsDigits + d] = run;
+      run += v[i];
+    }
+  }
+  for (int c = c0 + 8; c < c0 + per && c < chunks; ++c) {
+    base[c * kRsDigits + d] = run;
+    run += sums[c * kRsDigits + d];
   }
 }
 
-// Stable scatter of one digit pass.  FIRST: keys are the raw input (encoded
-// here) and the indices are the positions; LAST: the keys written are decoded
-// back to the input bits.
+// Stable scatter of one digit pass over chunk blockIdx.x.  FIRST: keys are
+// the raw input (encoded here) and the indices are the positions; LAST: the
+// keys written are decoded back to the input bits.
 template <typename K, int CODEC, bool FIRST, bool LAST>
-__global__ void __launch_bounds__(kRsThreads) rs_scatter_kernel(const K* __restrict__ in_keys,
+__global__ void __launch_bounds__(kRsThreads, 3) rs_scatter_kernel(const K* __restrict__ in_keys,
                                                                 const int* __restrict__ in_idx, K* __restrict__ out_keys,
-                                                                int* __restrict__ out_idx, const int* __restrict__ offs,
+                                                                int* __restrict__ out_idx, const int* __restrict__ base,
                                                                 int64_t n, int shift, int64_t num_tiles) {
   __shared__ K s_keys[kRsTile];
   __shared__ int s_idx[kRsTile];
   __shared__ int s_wh[kRsWarps][kRsDigits];  // per-warp running counts, then per-warp bases
   __shared__ int s_start[kRsDigits];         // first local position of each digit
-  __shared__ int s_goff[kRsDigits];          // global position of the tile's first key of each digit
+  __shared__ int s_delta[kRsDigits];         // output position minus local position, per digit
   __shared__ int sw[kRsWarps];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const unsigned lt = (1u << lane) - 1u;
-  for (int64_t t = blockIdx.x; t < num_tiles; t += gridDim.x) {
-    const int64_t t0 = t * kRsTile;
+  const int64_t tpc = chunk_tiles(num_tiles, gridDim.x);
+  int64_t t_hi = (blockIdx.x + 1) * tpc;
+  t_hi = t_hi < num_tiles ? t_hi : num_tiles;
+  int goff = base[blockIdx.x * kRsDigits + threadIdx.x];  // thread d: output position of digit d's next key
+  for (int64_t t = blockIdx.x * tpc; t < t_hi; ++t) {
+    const int t0 = (int)(t * kRsTile);  // n < 2^31: 32-bit positions
     const int valid = (int)(n - t0 < kRsTile ? n - t0 : kRsTile);
 #pragma unroll
     for (int k = 0; k < kRsWarps; ++k) s_wh[k][threadIdx.x] = 0;
-    s_goff[threadIdx.x] = offs[t * kRsDigits + threadIdx.x];
     __syncthreads();
     K kr[kRsEpt];
     int ir[kRsEpt], rk[kRsEpt];
@@ -185,7 +269,7 @@ __global__ void __launch_bounds__(kRsThreads) rs_scatter_kernel(const K* __restr
         K k = in_keys[t0 + e];
         if constexpr (FIRST) k = key_enc<K, CODEC>(k);
         kr[j] = k;
-        ir[j] = FIRST ? (int)(t0 + e) : in_idx[t0 + e];
+        ir[j] = FIRST ? t0 + e : in_idx[t0 + e];
       } else {
         kr[j] = (K)~(K)0;
         ir[j] = 0;
@@ -194,28 +278,31 @@ __global__ void __launch_bounds__(kRsThreads) rs_scatter_kernel(const K* __restr
 #pragma unroll
     for (int j = 0; j < kRsEpt; ++j) {
       const int d = (kr[j] >> shift) & 0xFF;
-      const unsigned peers = __match_any_sync(0xffffffffu, d);
+      const unsigned peers = digit_peers(d);
       const int r = __popc(peers & lt);
-      const int base = s_wh[w][d];
+      const int last = 31 - __clz(peers);
+      // every lane's read has returned before any lane passes the shuffle,
+      // so the last peer's update below cannot overtake a peer's read
+      const int b0 = __shfl_sync(0xffffffffu, s_wh[w][d], last);
+      if (lane == last) s_wh[w][d] = b0 + r + 1;  // the last peer publishes the new count
       __syncwarp();
-      if (r == __popc(peers) - 1) s_wh[w][d] = base + r + 1;  // the last peer publishes the new count
-      __syncwarp();
-      rk[j] = base + r;
+      rk[j] = b0 + r;
     }
     __syncthreads();
     // thread d: per-warp bases of digit d, then the tile-local digit starts
-    {
-      const int d = threadIdx.x;
-      int c = 0;
+    const int d_own = threadIdx.x;
+    int c_own = 0;
 #pragma unroll
-      for (int k = 0; k < kRsWarps; ++k) {
-        const int v = s_wh[k][d];
-        s_wh[k][d] = c;
-        c += v;
-      }
-      int tot;
-      s_start[d] = block_excl_scan256(c, sw, &tot);
+    for (int k = 0; k < kRsWarps; ++k) {
+      const int v = s_wh[k][d_own];
+      s_wh[k][d_own] = c_own;
+      c_own += v;
     }
+    int tot;
+    const int start = block_excl_scan256(c_own, sw, &tot);
+    s_start[d_own] = start;
+    s_delta[d_own] = goff - start;
+    goff += c_own;
     __syncthreads();
 #pragma unroll
     for (int j = 0; j < kRsEpt; ++j) {
@@ -227,8 +314,7 @@ __global__ void __launch_bounds__(kRsThreads) rs_scatter_kernel(const K* __restr
     __syncthreads();
     for (int p = threadIdx.x; p < valid; p += kRsThreads) {
       const K k = s_keys[p];
-      const int d = (k >> shift) & 0xFF;
-      const int g = s_goff[d] + (p - s_start[d]);
+      const int g = s_delta[(k >> shift) & 0xFF] + p;
       out_keys[g] = LAST ? key_dec<K, CODEC>(k) : k;
       out_idx[g] = s_idx[p];
     }
@@ -264,27 +350,53 @@ struct TopkState {
 };
 static_assert(sizeof(TopkState) == 64, "state");
 
-// 256-bin histogram of the key's high byte (LEVEL 0), or of the low byte
-// among keys whose high byte is st->hi (LEVEL 1); bins must be zero on entry.
-template <int CODEC, int LEVEL>
-__global__ void __launch_bounds__(kRsThreads) topk_hist_kernel(const uint16_t* __restrict__ x, int64_t n,
-                                                               const TopkState* __restrict__ st,
-                                                               unsigned* __restrict__ bins) {
-  __shared__ int s_h[kRsWarps][kRsDigits];
-  const int w = threadIdx.x >> 5;
+// 16 consecutive elements from e0 (16-byte vector loads when VEC and the
+// run is inside the array; elements past the end read as 0).
+template <bool VEC>
+__device__ __forceinline__ void load16(const uint16_t* __restrict__ x, int64_t e0, int64_t n, uint16_t (&v)[16]) {
+  if (VEC && e0 + 16 <= n) {
+    const uint4 a = __ldg(reinterpret_cast<const uint4*>(x + e0));
+    const uint4 b = __ldg(reinterpret_cast<const uint4*>(x + e0) + 1);
+    const uint32_t w[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
 #pragma unroll
-  for (int k = 0; k < kRsWarps; ++k) s_h[k][threadIdx.x] = 0;
-  __syncthreads();
-  const int hi = LEVEL ? st->hi : 0;
-  for (int64_t e = blockIdx.x * (int64_t)kRsThreads + threadIdx.x; e < n; e += (int64_t)gridDim.x * kRsThreads) {
-    const uint32_t k = topk_key<CODEC>(x[e]);
-    if (LEVEL == 0) atomicAdd(&s_h[w][k >> 8], 1);
-    else if ((int)(k >> 8) == hi) atomicAdd(&s_h[w][k & 0xFF], 1);
+    for (int i = 0; i < 8; ++i) {
+      v[2 * i] = (uint16_t)(w[i] & 0xFFFFu);
+      v[2 * i + 1] = (uint16_t)(w[i] >> 16);
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = e0 + i < n ? x[e0 + i] : (uint16_t)0;
   }
-  __syncthreads();
-  int c = 0;
+}
+
+template <int CODEC, int LEVEL>
+struct TopkDigit {
+  int hi;
+  __device__ __forceinline__ int operator()(uint16_t b) const {
+    const uint32_t k = topk_key<CODEC>(b);
+    if (LEVEL == 0) return (int)(k >> 8);
+    return (int)(k >> 8) == hi ? (int)(k & 0xFF) : -1;
+  }
+};
+
+// 256-bin histogram of the key's high byte (LEVEL 0), or of the low byte
+// among keys whose high byte is st->hi (LEVEL 1), over contiguous chunks of
+// tiles; bins must be zero on entry.
+template <int CODEC, int LEVEL, bool VEC>
+__global__ void __launch_bounds__(kRsThreads) topk_hist_kernel(const uint16_t* __restrict__ x, int64_t n,
+                                                               int64_t num_tiles, const TopkState* __restrict__ st,
+                                                               unsigned* __restrict__ bins) {
+  __shared__ int s_h[kHistCopies * kRsDigits];
 #pragma unroll
-  for (int k = 0; k < kRsWarps; ++k) c += s_h[k][threadIdx.x];
+  for (int k = 0; k < kHistCopies; ++k) s_h[k * kRsDigits + threadIdx.x] = 0;
+  __syncthreads();
+  const int64_t tpc = chunk_tiles(num_tiles, gridDim.x);
+  const int64_t e_lo = blockIdx.x * tpc * kRsTile;
+  int64_t e_hi = e_lo + tpc * kRsTile;
+  e_hi = e_hi < n ? e_hi : n;
+  smem_hist_range<uint16_t, VEC>(x, e_lo, e_hi, s_h, TopkDigit<CODEC, LEVEL>{LEVEL ? st->hi : 0});
+  __syncthreads();
+  const int c = smem_hist_total(s_h);
   if (c) atomicAdd(&bins[threadIdx.x], (unsigned)c);
 }
 
@@ -318,30 +430,34 @@ __global__ void __launch_bounds__(kRsThreads) topk_pick_kernel(const unsigned* _
 }
 
 // Per tile: elements above thr and equal to thr.
-template <int CODEC>
+template <int CODEC, bool VEC>
 __global__ void __launch_bounds__(kRsThreads) topk_count_kernel(const uint16_t* __restrict__ x, int64_t n,
                                                                 int64_t num_tiles, const TopkState* __restrict__ st,
                                                                 int* __restrict__ c_above, int* __restrict__ c_tie) {
-  __shared__ int sw[kRsWarps];
+  __shared__ int s_c[2][kRsWarps];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const uint32_t thr = (uint32_t)st->thr;
-  for (int64_t t = blockIdx.x; t < num_tiles; t += gridDim.x) {
-    const int64_t t0 = t * kRsTile;
-    int a = 0, q = 0;
+  int par = 0;
+  for (int64_t t = blockIdx.x; t < num_tiles; t += gridDim.x, par ^= 1) {
+    const int64_t e0 = t * kRsTile + (int64_t)threadIdx.x * kRsEpt;
+    uint16_t v[16];
+    load16<VEC>(x, e0, n, v);
+    int aq = 0;  // above in the low half, equal in the high half
 #pragma unroll
-    for (int j = 0; j < kRsEpt; ++j) {
-      const int64_t e = t0 + j * kRsThreads + threadIdx.x;
-      if (e < n) {
-        const uint32_t k = topk_key<CODEC>(x[e]);
-        a += k > thr;
-        q += k == thr;
-      }
+    for (int j = 0; j < 16; ++j) {
+      const uint32_t k = topk_key<CODEC>(v[j]);
+      const bool in = e0 + j < n;
+      aq += (in && k > thr) ? 1 : ((in && k == thr) ? 0x10000 : 0);
     }
-    int ta, tq;
-    block_excl_scan256(a, sw, &ta);
-    block_excl_scan256(q, sw, &tq);
+    aq = warp_sum_any(aq);
+    if (lane == 0) s_c[par][w] = aq;
+    __syncthreads();  // alternating slots: one barrier per tile
     if (threadIdx.x == 0) {
-      c_above[t] = ta;
-      c_tie[t] = tq;
+      int tot = 0;
+#pragma unroll
+      for (int k = 0; k < kRsWarps; ++k) tot += s_c[par][k];
+      c_above[t] = tot & 0xFFFF;
+      c_tie[t] = tot >> 16;
     }
   }
 }
@@ -385,7 +501,7 @@ __global__ void __launch_bounds__(kRsThreads) topk_offsets_kernel(const int* __r
 
 // Emits the selected elements of every tile in index order (values and int32
 // positions).  Tiles with nothing selected are skipped without reading them.
-template <int CODEC>
+template <int CODEC, bool VEC>
 __global__ void __launch_bounds__(kRsThreads) topk_emit_kernel(const uint16_t* __restrict__ x, int64_t n,
                                                                int64_t num_tiles, const TopkState* __restrict__ st,
                                                                const int* __restrict__ tie_before,
@@ -398,32 +514,27 @@ __global__ void __launch_bounds__(kRsThreads) topk_emit_kernel(const uint16_t* _
     const int o0 = off[t];
     if (off[t + 1] == o0) continue;  // block-uniform
     const int64_t e0 = t * kRsTile + (int64_t)threadIdx.x * kRsEpt;  // 16 consecutive elements per thread
-    uint32_t kk[kRsEpt];
-    uint16_t xv[kRsEpt];
-    int q = 0;
+    uint16_t xv[16];
+    load16<VEC>(x, e0, n, xv);
+    unsigned am = 0, qm = 0;
 #pragma unroll
-    for (int j = 0; j < kRsEpt; ++j) {
+    for (int j = 0; j < 16; ++j) {
+      const uint32_t kk = topk_key<CODEC>(xv[j]);
       const bool in = e0 + j < n;
-      xv[j] = in ? x[e0 + j] : (uint16_t)0;
-      kk[j] = in ? topk_key<CODEC>(xv[j]) : 0u;
-      q += in && kk[j] == thr;
+      am |= (unsigned)(in && kk > thr) << j;
+      qm |= (unsigned)(in && kk == thr) << j;
     }
     int tot;
-    int tr = tie_before[t] + block_excl_scan256(q, sw, &tot);  // tie rank of this thread's first tie
-    unsigned selm = 0;
-#pragma unroll
-    for (int j = 0; j < kRsEpt; ++j) {
-      const bool in = e0 + j < n;
-      bool s = in && kk[j] > thr;
-      if (in && kk[j] == thr) {
-        s = tr < ties;
-        ++tr;
-      }
-      selm |= (unsigned)s << j;
-    }
+    // ties of this thread that are still wanted: the first (ties - rank) of them
+    const int tr = tie_before[t] + block_excl_scan256(__popc(qm), sw, &tot);
+    int want = ties - tr;
+    want = want < 0 ? 0 : want;
+    unsigned take = qm;
+    for (int c = __popc(qm); c > want; --c) take &= ~(1u << (31 - __clz(take)));  // drop the last ties
+    const unsigned selm = am | take;
     int o = o0 + block_excl_scan256(__popc(selm), sw, &tot);
 #pragma unroll
-    for (int j = 0; j < kRsEpt; ++j) {
+    for (int j = 0; j < 16; ++j) {
       if (((selm >> j) & 1u) && o < k) {
         out[o] = xv[j];
         idx_out[o] = (int)(e0 + j);
@@ -490,29 +601,31 @@ static int64_t rs_tiles(int64_t n) { return (n + kRsTile - 1) / kRsTile; }
 
 static size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
-// tmp layout: keys[n] (K) | idx[n] (int32) | counts[tiles * 256] | offs[tiles * 256] | totals[256]
-static size_t rs_tmp_bytes(int key_bytes, int64_t n) {
-  const int64_t T = rs_tiles(n);
-  return align256((size_t)n * key_bytes) + align256((size_t)n * 4) + 2 * align256((size_t)T * kRsDigits * 4) +
-         align256(kRsDigits * 4);
+// tmp layout: keys[n] (K) | idx[n] (int32) | sums[chunks * 256] | base[chunks * 256] | totals[256]
+constexpr int kRsChunksPerSm = 3;  // the scatter kernel holds 3 CTAs per SM
+
+static int rs_chunks(int64_t tiles) {
+  int64_t c = (int64_t)sm_count() * kRsChunksPerSm;
+  if (tiles < c) c = tiles;
+  return (int)(c < 1 ? 1 : c);
 }
 
-static int rs_grid(int64_t tiles, int per_sm) {
-  int64_t g = (int64_t)sm_count() * per_sm;
-  if (tiles < g) g = tiles;
-  return (int)(g < 1 ? 1 : g);
+static size_t rs_tmp_bytes(int key_bytes, int64_t n) {
+  const int C = rs_chunks(rs_tiles(n));
+  return align256((size_t)n * key_bytes) + align256((size_t)n * 4) + 2 * align256((size_t)C * kRsDigits * 4) +
+         align256(kRsDigits * 4);
 }
 
 template <typename K, int CODEC>
 static tcu_status_t radix_sort_t(const K* x, int64_t n, K* out, int* idx_out, uint8_t* tmp, cudaStream_t st) {
   const int64_t T = rs_tiles(n);
+  const int C = rs_chunks(T);
   K* tk = reinterpret_cast<K*>(tmp);
   int* ti = reinterpret_cast<int*>(tmp + align256((size_t)n * sizeof(K)));
-  int* counts = reinterpret_cast<int*>(reinterpret_cast<uint8_t*>(ti) + align256((size_t)n * 4));
-  int* offs = reinterpret_cast<int*>(reinterpret_cast<uint8_t*>(counts) + align256((size_t)T * kRsDigits * 4));
-  unsigned* totals = reinterpret_cast<unsigned*>(reinterpret_cast<uint8_t*>(offs) + align256((size_t)T * kRsDigits * 4));
+  int* sums = reinterpret_cast<int*>(reinterpret_cast<uint8_t*>(ti) + align256((size_t)n * 4));
+  int* base = reinterpret_cast<int*>(reinterpret_cast<uint8_t*>(sums) + align256((size_t)C * kRsDigits * 4));
+  unsigned* totals = reinterpret_cast<unsigned*>(reinterpret_cast<uint8_t*>(base) + align256((size_t)C * kRsDigits * 4));
   constexpr int passes = (int)sizeof(K);
-  const int g = rs_grid(T, 8);
   // ping-pong so that the last pass lands in out / idx_out
   const K* src_k = x;
   const int* src_i = nullptr;
@@ -521,26 +634,36 @@ static tcu_status_t radix_sort_t(const K* x, int64_t n, K* out, int* idx_out, ui
     const bool to_out = ((passes - 1 - p) % 2) == 0;
     K* dk = to_out ? out : tk;
     int* di = to_out ? idx_out : ti;
-    cudaError_t e = cudaMemsetAsync(totals, 0, kRsDigits * 4, st);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(radix totals)");
     const int shift = 8 * p;
-    if (p == 0) rs_hist_kernel<K, CODEC, true><<<g, kRsThreads, 0, st>>>(src_k, n, shift, T, counts, totals);
-    else rs_hist_kernel<K, CODEC, false><<<g, kRsThreads, 0, st>>>(src_k, n, shift, T, counts, totals);
-    rs_offsets_kernel<<<kRsDigits, kRsThreads, 0, st>>>(counts, totals, T, offs);
-    if (p == 0 && last)
-      rs_scatter_kernel<K, CODEC, true, true><<<g, kRsThreads, 0, st>>>(src_k, src_i, dk, di, offs, n, shift, T);
+    cudaError_t e1 = cudaMemsetAsync(totals, 0, kRsDigits * 4, st);
+    if (e1 != cudaSuccess) return cuda_fail(e1, "cudaMemsetAsync(radix totals)");
+    if (p == 0 && aligned16(src_k))
+      rs_hist_kernel<K, CODEC, true, true><<<C, kRsThreads, 0, st>>>(src_k, n, shift, T, sums, totals);
     else if (p == 0)
-      rs_scatter_kernel<K, CODEC, true, false><<<g, kRsThreads, 0, st>>>(src_k, src_i, dk, di, offs, n, shift, T);
+      rs_hist_kernel<K, CODEC, true, false><<<C, kRsThreads, 0, st>>>(src_k, n, shift, T, sums, totals);
+    else  // the scratch and output buffers are 16-byte aligned
+      rs_hist_kernel<K, CODEC, false, true><<<C, kRsThreads, 0, st>>>(src_k, n, shift, T, sums, totals);
+    rs_chunk_scan_kernel<<<kRsDigits, kChunkScanThreads, 0, st>>>(sums, C, totals, base);
+    if (p == 0 && last)
+      rs_scatter_kernel<K, CODEC, true, true><<<C, kRsThreads, 0, st>>>(src_k, src_i, dk, di, base, n, shift, T);
+    else if (p == 0)
+      rs_scatter_kernel<K, CODEC, true, false><<<C, kRsThreads, 0, st>>>(src_k, src_i, dk, di, base, n, shift, T);
     else if (last)
-      rs_scatter_kernel<K, CODEC, false, true><<<g, kRsThreads, 0, st>>>(src_k, src_i, dk, di, offs, n, shift, T);
+      rs_scatter_kernel<K, CODEC, false, true><<<C, kRsThreads, 0, st>>>(src_k, src_i, dk, di, base, n, shift, T);
     else
-      rs_scatter_kernel<K, CODEC, false, false><<<g, kRsThreads, 0, st>>>(src_k, src_i, dk, di, offs, n, shift, T);
-    e = cudaGetLastError();
+      rs_scatter_kernel<K, CODEC, false, false><<<C, kRsThreads, 0, st>>>(src_k, src_i, dk, di, base, n, shift, T);
+    cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "radix sort launch");
     src_k = dk;
     src_i = di;
   }
   return TCU_OK;
+}
+
+static int rs_grid(int64_t tiles, int per_sm) {
+  int64_t g = (int64_t)sm_count() * per_sm;
+  if (tiles < g) g = tiles;
+  return (int)(g < 1 ? 1 : g);
 }
 
 // tmp layout: bins[2][256] | state | c_above[T] | c_tie[T] | tie_before[T] | off[T + 1]
@@ -552,6 +675,7 @@ static size_t topk_tmp_bytes(int64_t n) {
 template <int CODEC>
 static tcu_status_t topk_t(const uint16_t* x, int64_t n, int64_t k, uint16_t* out, int* idx_out, uint8_t* tmp,
                            cudaStream_t st) {
+  const bool VEC = aligned16(x);
   const int64_t T = rs_tiles(n);
   unsigned* bins = reinterpret_cast<unsigned*>(tmp);
   TopkState* state = reinterpret_cast<TopkState*>(tmp + 2048);
@@ -561,18 +685,25 @@ static tcu_status_t topk_t(const uint16_t* x, int64_t n, int64_t k, uint16_t* ou
   int* off = reinterpret_cast<int*>(reinterpret_cast<uint8_t*>(tie_before) + align256((size_t)T * 4));
   cudaError_t e = cudaMemsetAsync(tmp, 0, 2048 + sizeof(TopkState), st);
   if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(topk state)");
-  int64_t hg = (n + kRsThreads * 16 - 1) / (kRsThreads * 16);
-  const int64_t hcap = (int64_t)sm_count() * 8;
-  if (hg > hcap) hg = hcap;
-  if (hg < 1) hg = 1;
-  topk_hist_kernel<CODEC, 0><<<(int)hg, kRsThreads, 0, st>>>(x, n, state, bins);
-  topk_pick_kernel<0><<<1, kRsThreads, 0, st>>>(bins, k, state);
-  topk_hist_kernel<CODEC, 1><<<(int)hg, kRsThreads, 0, st>>>(x, n, state, bins + 256);
-  topk_pick_kernel<1><<<1, kRsThreads, 0, st>>>(bins + 256, k, state);
   const int g = rs_grid(T, 8);
-  topk_count_kernel<CODEC><<<g, kRsThreads, 0, st>>>(x, n, T, state, c_above, c_tie);
-  topk_offsets_kernel<<<1, kRsThreads, 0, st>>>(c_above, c_tie, T, state, tie_before, off);
-  topk_emit_kernel<CODEC><<<g, kRsThreads, 0, st>>>(x, n, T, state, tie_before, off, k, out, idx_out);
+  const int gh = rs_grid(T, 3);  // histogram CTAs hold 64 KB of counters
+  if (VEC) {
+    topk_hist_kernel<CODEC, 0, true><<<gh, kRsThreads, 0, st>>>(x, n, T, state, bins);
+    topk_pick_kernel<0><<<1, kRsThreads, 0, st>>>(bins, k, state);
+    topk_hist_kernel<CODEC, 1, true><<<gh, kRsThreads, 0, st>>>(x, n, T, state, bins + 256);
+    topk_pick_kernel<1><<<1, kRsThreads, 0, st>>>(bins + 256, k, state);
+    topk_count_kernel<CODEC, true><<<g, kRsThreads, 0, st>>>(x, n, T, state, c_above, c_tie);
+    topk_offsets_kernel<<<1, kRsThreads, 0, st>>>(c_above, c_tie, T, state, tie_before, off);
+    topk_emit_kernel<CODEC, true><<<g, kRsThreads, 0, st>>>(x, n, T, state, tie_before, off, k, out, idx_out);
+  } else {
+    topk_hist_kernel<CODEC, 0, false><<<gh, kRsThreads, 0, st>>>(x, n, T, state, bins);
+    topk_pick_kernel<0><<<1, kRsThreads, 0, st>>>(bins, k, state);
+    topk_hist_kernel<CODEC, 1, false><<<gh, kRsThreads, 0, st>>>(x, n, T, state, bins + 256);
+    topk_pick_kernel<1><<<1, kRsThreads, 0, st>>>(bins + 256, k, state);
+    topk_count_kernel<CODEC, false><<<g, kRsThreads, 0, st>>>(x, n, T, state, c_above, c_tie);
+    topk_offsets_kernel<<<1, kRsThreads, 0, st>>>(c_above, c_tie, T, state, tie_before, off);
+    topk_emit_kernel<CODEC, false><<<g, kRsThreads, 0, st>>>(x, n, T, state, tie_before, off, k, out, idx_out);
+  }
   e = cudaGetLastError();
   return e == cudaSuccess ? TCU_OK : cuda_fail(e, "topk launch");
 }
