@@ -232,31 +232,81 @@ __global__ void __launch_bounds__(kChunkScanThreads) rs_chunk_scan_kernel(const 
   }
 }
 
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc, int src_bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(smem_dst)), "l"(gsrc), "r"(src_bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
+// Copies `bytes` bytes from g to s with 16-byte cp.async chunks spread over
+// the block (the last chunk zero-filled past `bytes`).
+__device__ __forceinline__ void cp_async_block(void* s, const void* g, int bytes) {
+  for (int c = threadIdx.x; c * 16 < bytes; c += kRsThreads) {
+    const int sz = bytes - 16 * c < 16 ? bytes - 16 * c : 16;
+    cp_async16(static_cast<uint8_t*>(s) + 16 * c, static_cast<const uint8_t*>(g) + 16 * c, sz);
+  }
+}
+
+template <typename K>
+struct ScatterSmem {
+  static constexpr int BUF = kRsTile * ((int)sizeof(K) + 4);  // keys then indices of one tile
+  static constexpr int WH = 2 * BUF;                           // per-warp digit counts
+  static constexpr int START = WH + kRsWarps * kRsDigits * 4;
+  static constexpr int DELTA = START + kRsDigits * 4;
+  static constexpr int SW = DELTA + kRsDigits * 4;
+  static constexpr int BYTES = SW + kRsWarps * 4;
+};
+
 // Stable scatter of one digit pass over chunk blockIdx.x.  FIRST: keys are
 // the raw input (encoded here) and the indices are the positions; LAST: the
-// keys written are decoded back to the input bits.
-template <typename K, int CODEC, bool FIRST, bool LAST>
+// keys written are decoded back to the input bits.  ASYNC (inputs 16-byte
+// aligned): the next tile's keys and indices are copied into the other of
+// two shared buffers with cp.async while the current tile is ranked; the
+// current buffer then takes the tile sorted by digit.  Dynamic shared memory:
+// ScatterSmem<K>::BYTES.
+template <typename K, int CODEC, bool FIRST, bool LAST, bool ASYNC>
 __global__ void __launch_bounds__(kRsThreads, 3) rs_scatter_kernel(const K* __restrict__ in_keys,
-                                                                const int* __restrict__ in_idx, K* __restrict__ out_keys,
-                                                                int* __restrict__ out_idx, const int* __restrict__ base,
-                                                                int64_t n, int shift, int64_t num_tiles) {
-  __shared__ K s_keys[kRsTile];
-  __shared__ int s_idx[kRsTile];
-  __shared__ int s_wh[kRsWarps][kRsDigits];  // per-warp running counts, then per-warp bases
-  __shared__ int s_start[kRsDigits];         // first local position of each digit
-  __shared__ int s_delta[kRsDigits];         // output position minus local position, per digit
-  __shared__ int sw[kRsWarps];
+                                                                   const int* __restrict__ in_idx,
+                                                                   K* __restrict__ out_keys, int* __restrict__ out_idx,
+                                                                   const int* __restrict__ base, int64_t n, int shift,
+                                                                   int64_t num_tiles) {
+  using L = ScatterSmem<K>;
+  extern __shared__ __align__(16) uint8_t sm[];
+  int(*s_wh)[kRsDigits] = reinterpret_cast<int(*)[kRsDigits]>(sm + L::WH);  // per-warp counts, then bases
+  int* s_start = reinterpret_cast<int*>(sm + L::START);  // first local position of each digit
+  int* s_delta = reinterpret_cast<int*>(sm + L::DELTA);  // output position minus local position, per digit
+  int* sw = reinterpret_cast<int*>(sm + L::SW);
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const unsigned lt = (1u << lane) - 1u;
   const int64_t tpc = chunk_tiles(num_tiles, gridDim.x);
   int64_t t_hi = (blockIdx.x + 1) * tpc;
   t_hi = t_hi < num_tiles ? t_hi : num_tiles;
+  const int64_t t_lo = blockIdx.x * tpc;
+  auto tile_valid = [&](int64_t t) { return (int)(n - t * kRsTile < kRsTile ? n - t * kRsTile : kRsTile); };
+  auto issue = [&](int64_t t, int b) {
+    const int t0 = (int)(t * kRsTile), v = tile_valid(t);
+    cp_async_block(sm + b * L::BUF, in_keys + t0, v * (int)sizeof(K));
+    if constexpr (!FIRST) cp_async_block(sm + b * L::BUF + kRsTile * (int)sizeof(K), in_idx + t0, v * 4);
+  };
   int goff = base[blockIdx.x * kRsDigits + threadIdx.x];  // thread d: output position of digit d's next key
-  for (int64_t t = blockIdx.x * tpc; t < t_hi; ++t) {
+  if (ASYNC && t_lo < t_hi) {
+    issue(t_lo, 0);
+    cp_async_commit();
+  }
+  int b = 0;
+  for (int64_t t = t_lo; t < t_hi; ++t, b ^= (ASYNC ? 1 : 0)) {
     const int t0 = (int)(t * kRsTile);  // n < 2^31: 32-bit positions
-    const int valid = (int)(n - t0 < kRsTile ? n - t0 : kRsTile);
+    const int valid = tile_valid(t);
+    K* bk = reinterpret_cast<K*>(sm + b * L::BUF);
+    int* bi = reinterpret_cast<int*>(sm + b * L::BUF + kRsTile * (int)sizeof(K));
 #pragma unroll
     for (int k = 0; k < kRsWarps; ++k) s_wh[k][threadIdx.x] = 0;
+    if constexpr (ASYNC) {
+      if (t + 1 < t_hi) issue(t + 1, b ^ 1);  // that buffer was released by the last barrier of tile t - 1
+      cp_async_commit();
+      cp_async_wait1();  // this thread's copies of tile t have landed
+    }
     __syncthreads();
     K kr[kRsEpt];
     int ir[kRsEpt], rk[kRsEpt];
@@ -266,10 +316,10 @@ __global__ void __launch_bounds__(kRsThreads, 3) rs_scatter_kernel(const K* __re
     for (int j = 0; j < kRsEpt; ++j) {
       const int e = w * (kRsEpt * 32) + j * 32 + lane;
       if (e < valid) {
-        K k = in_keys[t0 + e];
+        K k = ASYNC ? bk[e] : in_keys[t0 + e];
         if constexpr (FIRST) k = key_enc<K, CODEC>(k);
         kr[j] = k;
-        ir[j] = FIRST ? t0 + e : in_idx[t0 + e];
+        ir[j] = FIRST ? t0 + e : (ASYNC ? bi[e] : in_idx[t0 + e]);
       } else {
         kr[j] = (K)~(K)0;
         ir[j] = 0;
@@ -288,7 +338,7 @@ __global__ void __launch_bounds__(kRsThreads, 3) rs_scatter_kernel(const K* __re
       __syncwarp();
       rk[j] = b0 + r;
     }
-    __syncthreads();
+    __syncthreads();  // also: the input buffer is no longer read
     // thread d: per-warp bases of digit d, then the tile-local digit starts
     const int d_own = threadIdx.x;
     int c_own = 0;
@@ -308,17 +358,17 @@ __global__ void __launch_bounds__(kRsThreads, 3) rs_scatter_kernel(const K* __re
     for (int j = 0; j < kRsEpt; ++j) {
       const int d = (kr[j] >> shift) & 0xFF;
       const int pos = s_start[d] + s_wh[w][d] + rk[j];
-      s_keys[pos] = kr[j];
-      s_idx[pos] = ir[j];
+      bk[pos] = kr[j];
+      bi[pos] = ir[j];
     }
     __syncthreads();
     for (int p = threadIdx.x; p < valid; p += kRsThreads) {
-      const K k = s_keys[p];
+      const K k = bk[p];
       const int g = s_delta[(k >> shift) & 0xFF] + p;
       out_keys[g] = LAST ? key_dec<K, CODEC>(k) : k;
-      out_idx[g] = s_idx[p];
+      out_idx[g] = bi[p];
     }
-    __syncthreads();  // the tile's shared arrays are reused by the next tile
+    __syncthreads();  // the buffer and the per-digit arrays are reused
   }
 }
 
@@ -616,6 +666,27 @@ static size_t rs_tmp_bytes(int key_bytes, int64_t n) {
          align256(kRsDigits * 4);
 }
 
+template <typename K, int CODEC, bool FIRST, bool LAST>
+static cudaError_t launch_scatter(bool async_ok, int C, cudaStream_t st, const K* src_k, const int* src_i, K* dk, int* di,
+                                  const int* base, int64_t n, int shift, int64_t T) {
+  constexpr int smem = ScatterSmem<K>::BYTES;
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(rs_scatter_kernel<K, CODEC, FIRST, LAST, true>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(rs_scatter_kernel<K, CODEC, FIRST, LAST, false>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  if (async_ok)
+    rs_scatter_kernel<K, CODEC, FIRST, LAST, true><<<C, kRsThreads, smem, st>>>(src_k, src_i, dk, di, base, n, shift, T);
+  else
+    rs_scatter_kernel<K, CODEC, FIRST, LAST, false><<<C, kRsThreads, smem, st>>>(src_k, src_i, dk, di, base, n, shift, T);
+  return cudaGetLastError();
+}
+
 template <typename K, int CODEC>
 static tcu_status_t radix_sort_t(const K* x, int64_t n, K* out, int* idx_out, uint8_t* tmp, cudaStream_t st) {
   const int64_t T = rs_tiles(n);
@@ -644,14 +715,12 @@ static tcu_status_t radix_sort_t(const K* x, int64_t n, K* out, int* idx_out, ui
     else  // the scratch and output buffers are 16-byte aligned
       rs_hist_kernel<K, CODEC, false, true><<<C, kRsThreads, 0, st>>>(src_k, n, shift, T, sums, totals);
     rs_chunk_scan_kernel<<<kRsDigits, kChunkScanThreads, 0, st>>>(sums, C, totals, base);
-    if (p == 0 && last)
-      rs_scatter_kernel<K, CODEC, true, true><<<C, kRsThreads, 0, st>>>(src_k, src_i, dk, di, base, n, shift, T);
-    else if (p == 0)
-      rs_scatter_kernel<K, CODEC, true, false><<<C, kRsThreads, 0, st>>>(src_k, src_i, dk, di, base, n, shift, T);
-    else if (last)
-      rs_scatter_kernel<K, CODEC, false, true><<<C, kRsThreads, 0, st>>>(src_k, src_i, dk, di, base, n, shift, T);
-    else
-      rs_scatter_kernel<K, CODEC, false, false><<<C, kRsThreads, 0, st>>>(src_k, src_i, dk, di, base, n, shift, T);
+    const bool async_ok = aligned16(src_k) && (p == 0 || aligned16(src_i));
+    if (p == 0 && last) e1 = launch_scatter<K, CODEC, true, true>(async_ok, C, st, src_k, src_i, dk, di, base, n, shift, T);
+    else if (p == 0) e1 = launch_scatter<K, CODEC, true, false>(async_ok, C, st, src_k, src_i, dk, di, base, n, shift, T);
+    else if (last) e1 = launch_scatter<K, CODEC, false, true>(async_ok, C, st, src_k, src_i, dk, di, base, n, shift, T);
+    else e1 = launch_scatter<K, CODEC, false, false>(async_ok, C, st, src_k, src_i, dk, di, base, n, shift, T);
+    if (e1 != cudaSuccess) return cuda_fail(e1, "radix scatter launch");
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "radix sort launch");
     src_k = dk;
