@@ -11,6 +11,8 @@ segmented sum), exactly where the reference also synchronises.
 S x S triangular tile multiplied on the tensor cores, one of 16, 32, 64, 128;
 ``None`` or 0 selects the autotuned value.
 """
+import os
+
 import torch
 
 from . import _lib
@@ -647,6 +649,25 @@ def _bounds_input(indptr, device, where):
     return indptr.contiguous()
 
 
+# Mean segment length up to which segment sums and SpMV take the element-split
+# SIMT kernels (tcu_seg_sum_rows / tcu_spmv_rows) instead of the tensor-core
+# segmented sum, which is bound by segment starts when segments are short.
+# Measured on B200 at 2^26 / 2^28 fp16 (CUDA-graph replays): the split path
+# is 3.7x faster at mean 4 and 1.2x at mean 16; the tensor cores are ahead
+# from mean 64 (0.14 vs 0.16 ms at 2^26).  SpMV on 2^20 Zipf(1.6) rows
+# (mean 16): 0.125 vs 0.228 ms.
+ROWS_MAX_MEAN = int(os.environ.get("TCU_ROWS_MAX_MEAN", "32"))
+
+
+def _use_rows(n, nseg):
+    return nseg > 0 and n <= ROWS_MAX_MEAN * nseg
+
+
+def _rows_ws(device, n):
+    """The stream's workspace, sized for the element-split row kernels."""
+    return workspace(device, _lib.lib.tcu_rows_workspace_bytes(n))
+
+
 def _seg_sum_bounds(x, bounds, S, where):
     x = _seg_x(x, where)
     bounds = _bounds_input(bounds, x.device, where)
@@ -655,6 +676,14 @@ def _seg_sum_bounds(x, bounds, S, where):
     if nb < 2:
         return out
     n = x.numel()
+    if _use_rows(n, nb - 1):
+        _check_S_opt(S)
+        ws, wsb = _rows_ws(x.device, n)
+        check(_lib.lib.tcu_seg_sum_rows(x.data_ptr(), _lib.DTYPE_CODE[x.dtype], n, bounds.data_ptr(),
+                                        _lib.DTYPE_CODE[bounds.dtype], nb, out.data_ptr(), ws, wsb,
+                                        stream_ptr(x.device)), where)
+        _after(x)
+        return out
     S = _pick_S(S, x.dtype, n, op="seg")
     ws, wsb = workspace(x.device, _lib.lib.tcu_workspace_bytes(n, S))
     st = _lib.lib.tcu_seg_bounds(x.data_ptr(), _lib.DTYPE_CODE[x.dtype], n, S, bounds.data_ptr(),
@@ -742,6 +771,14 @@ def _spmv(vals, indptr, cols, x, S, where):
     y = torch.empty(max(rows, 0), dtype=torch.float32, device=x.device)
     if rows <= 0:
         return y
+    if _use_rows(nnz, rows):
+        _check_S_opt(S)
+        ws, wsb = _rows_ws(x.device, nnz)
+        check(_lib.lib.tcu_spmv_rows(vals.data_ptr(), _lib.DTYPE_CODE[vals.dtype], indptr.data_ptr(),
+                                     _lib.DTYPE_CODE[indptr.dtype], rows, cols.data_ptr(), nnz, x.data_ptr(),
+                                     x.numel(), y.data_ptr(), ws, wsb, stream_ptr(x.device)), where)
+        _after(x)
+        return y
     prod = torch.empty(max((nnz + 63) // 64 * 64, 64), dtype=torch.float32, device=x.device)  # pre-split rows
     S = _pick_S(S, torch.float32, nnz, op="seg")
     ws, wsb = workspace(x.device, _lib.lib.tcu_workspace_bytes(nnz, S))
@@ -757,10 +794,11 @@ def run_spmv_v2(vals, indptr, cols, x, s, segm_offsets=None):
     """y = A x for CSR (vals, indptr, cols) (reference: src/torch/torch_spmv.h:112-209).
 
     vals and x both fp16 or both fp32; y is fp32.  Products are formed in fp32
-    (the reference rounds fp16 products to fp16 first) and summed per row by
-    the tensor-core segmented sum (split-precision bf16 hi + lo, FP64 carries
-    for rows spanning tiles).  ``segm_offsets`` is accepted for signature
-    compatibility and not read."""
+    (the reference rounds fp16 products to fp16 first).  Short rows (mean
+    nnz per row <= ROWS_MAX_MEAN) are summed by the element-split SIMT kernel
+    in FP32; longer rows by the tensor-core segmented sum (split-precision
+    bf16 hi + lo, FP64 carries for rows spanning tiles).  ``segm_offsets`` is
+    accepted for signature compatibility and not read."""
     return _spmv(vals, indptr, cols, x, s, "run_spmv_v2")
 
 

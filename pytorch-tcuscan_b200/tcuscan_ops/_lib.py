@@ -81,6 +81,9 @@ _sig("tcu_mask_count", _ST, _P, _I64, _P, _P)
 _sig("tcu_compress_count", _ST, _P, _I64, _I, _I, _I, _P, _P, _SZ, _P)
 _sig("tcu_compress_counted", _ST, _P, _I, _P, _I64, _P, _I, _I, _P, _P, _I64, _P, _SZ, _P)
 _sig("tcu_compress_segments", _ST, _P, _I, _P, _I64, _P, _I64, _P, _I64, _P, _P, _SZ, _P)
+_sig("tcu_rows_workspace_bytes", _SZ, _I64)
+_sig("tcu_seg_sum_rows", _ST, _P, _I, _I64, _P, _I, _I64, _P, _P, _SZ, _P)
+_sig("tcu_spmv_rows", _ST, _P, _I, _P, _I, _I64, _P, _I64, _P, _I64, _P, _P, _SZ, _P)
 _sig("tcu_split", _ST, _P, _I, _P, _I64, _P, _I, _I, _P, _P, _P, _P, _SZ, _P)
 _sig("tcu_radix_sort_tmp_bytes", _SZ, _I, _I64)
 _sig("tcu_radix_sort", _ST, _P, _I, _I64, _P, _P, _P, _SZ, _P)
