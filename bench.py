@@ -442,7 +442,8 @@ def measure_serving(dev, count=20000, seed=11, sample=240):
     srv = serve.Server(dev, budget_bytes=24 << 30, slots=4, keep_results=True)
     srv.submit_many(*wl.arrays(idx), np.zeros(idx.size))
     srv.run()
-    exact_ok, err_srv, err_one, diff = True, 0.0, 0.0, 0.0
+    exact_ok = True
+    err_srv, err_one, diff = {}, {}, {}  # per float dtype
 
     def fp64_ref(op, x, aux):
         if op == serve.SCAN:
@@ -466,9 +467,10 @@ def measure_serving(dev, count=20000, seed=11, sample=240):
                 exact_ok &= bool(torch.equal(got.long(), fp64_ref(op, x, aux).long().to(got.dtype).long()))
         else:
             r = fp64_ref(op, x, aux)
-            err_srv = max(err_srv, rel(got, r))
-            err_one = max(err_one, rel(one, r))
-            diff = max(diff, rel(got, one.double()))
+            dk = str(x.dtype).replace("torch.", "")
+            err_srv[dk] = max(err_srv.get(dk, 0.0), rel(got, r))
+            err_one[dk] = max(err_one.get(dk, 0.0), rel(one, r))
+            diff[dk] = max(diff.get(dk, 0.0), rel(got, one.double()))
     srv.release()
     out["sample_checked"] = int(idx.size)
     out["sample_integer_results_identical"] = exact_ok

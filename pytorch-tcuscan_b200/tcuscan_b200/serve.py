@@ -130,7 +130,8 @@ class Server:
         self.keep = bool(keep_results)
         self.timing = bool(timing)
         # per-slot look-back workspace sized for the largest batch, then the arena
-        ws_need = int(_lib.lib.tcu_workspace_bytes(self.max_batch_bytes, 64))
+        ws_need = int(max(_lib.lib.tcu_workspace_bytes(self.max_batch_bytes, 64),
+                          _lib.lib.tcu_rows_workspace_bytes(self.max_batch_bytes)))
         self.slots = []
         for i in range(slots):
             sl = _Slot()
@@ -461,8 +462,12 @@ class Server:
                 iw = int(self.iw[ids[0]])
                 tcuscan_ops.check(L.tcu_pack(base + m_off + items.nbytes, k, iw, 8, base + b_off, nbt, sp),
                                   "serve pack row pointers")
-                s_ = L.tcu_seg_bounds(base + x_off, _lib.DTYPE_CODE[dtype], total, S, base + b_off, _lib.TCU_INT64,
-                                      nbt, 1, base + z_off, sl.ws.data_ptr(), sl.wsb, sp)
+                if tcuscan_ops._rows_for(dtype, total, nbt - 1):  # same rule as run_seg_sum_*
+                    s_ = L.tcu_seg_sum_rows(base + x_off, _lib.DTYPE_CODE[dtype], total, base + b_off,
+                                            _lib.TCU_INT64, nbt, base + z_off, sl.ws.data_ptr(), sl.wsb, sp)
+                else:
+                    s_ = L.tcu_seg_bounds(base + x_off, _lib.DTYPE_CODE[dtype], total, S, base + b_off,
+                                          _lib.TCU_INT64, nbt, 1, base + z_off, sl.ws.data_ptr(), sl.wsb, sp)
                 tcuscan_ops.check(s_, "serve seg_sum")
                 self.roff[ids], self.rlen[ids] = boff, self.nseg[ids]
                 out_len = max(nbt - 1, 1)

@@ -663,6 +663,20 @@ def _use_rows(n, nseg):
     return nseg > 0 and n <= ROWS_MAX_MEAN * nseg
 
 
+# float32 segment sums (and SpMV, whose products are float32) always take
+# the element-split path: the tensor-core form takes segment sums as
+# differences of bf16 hi + lo prefix sums, which carry ~1e-3 absolute error
+# from the split representation accumulated along the prefix, while the split
+# path sums in FP32; for SpMV it is also the faster one at every row length
+# (both are bound by the x gathers).
+ROWS_FP32 = True
+
+
+def _rows_for(dtype, n, nseg):
+    """Whether segment sums of `dtype` take the element-split path."""
+    return nseg > 0 and ((ROWS_FP32 and dtype == torch.float32) or _use_rows(n, nseg))
+
+
 def _rows_ws(device, n):
     """The stream's workspace, sized for the element-split row kernels."""
     return workspace(device, _lib.lib.tcu_rows_workspace_bytes(n))
@@ -676,7 +690,7 @@ def _seg_sum_bounds(x, bounds, S, where):
     if nb < 2:
         return out
     n = x.numel()
-    if _use_rows(n, nb - 1):
+    if _rows_for(x.dtype, n, nb - 1):
         _check_S_opt(S)
         ws, wsb = _rows_ws(x.device, n)
         check(_lib.lib.tcu_seg_sum_rows(x.data_ptr(), _lib.DTYPE_CODE[x.dtype], n, bounds.data_ptr(),
@@ -771,7 +785,7 @@ def _spmv(vals, indptr, cols, x, S, where):
     y = torch.empty(max(rows, 0), dtype=torch.float32, device=x.device)
     if rows <= 0:
         return y
-    if _use_rows(nnz, rows):
+    if _rows_for(torch.float32, nnz, rows):
         _check_S_opt(S)
         ws, wsb = _rows_ws(x.device, nnz)
         check(_lib.lib.tcu_spmv_rows(vals.data_ptr(), _lib.DTYPE_CODE[vals.dtype], indptr.data_ptr(),
@@ -794,11 +808,11 @@ def run_spmv_v2(vals, indptr, cols, x, s, segm_offsets=None):
     """y = A x for CSR (vals, indptr, cols) (reference: src/torch/torch_spmv.h:112-209).
 
     vals and x both fp16 or both fp32; y is fp32.  Products are formed in fp32
-    (the reference rounds fp16 products to fp16 first).  Short rows (mean
-    nnz per row <= ROWS_MAX_MEAN) are summed by the element-split SIMT kernel
-    in FP32; longer rows by the tensor-core segmented sum (split-precision
-    bf16 hi + lo, FP64 carries for rows spanning tiles).  ``segm_offsets`` is
-    accepted for signature compatibility and not read."""
+    (the reference rounds fp16 products to fp16 first) and summed per row in
+    FP32 by the element-split SIMT kernel (tcu_spmv_rows); with ROWS_FP32 off
+    they go to the tensor-core segmented sum instead (tcu_spmv_csr:
+    split-precision bf16 hi + lo, FP64 carries for rows spanning tiles).
+    ``segm_offsets`` is accepted for signature compatibility and not read."""
     return _spmv(vals, indptr, cols, x, s, "run_spmv_v2")
 
 
