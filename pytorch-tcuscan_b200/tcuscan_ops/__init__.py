@@ -669,7 +669,7 @@ def _use_rows(n, nseg):
 # from the split representation accumulated along the prefix, while the split
 # path sums in FP32; for SpMV it is also the faster one at every row length
 # (both are bound by the x gathers).
-ROWS_FP32 = True
+ROWS_FP32 = os.environ.get("TCU_ROWS_FP32", "1") != "0"
 
 
 def _rows_for(dtype, n, nseg):
