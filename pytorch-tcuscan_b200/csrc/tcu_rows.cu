@@ -32,8 +32,8 @@ namespace tcu {
 
 constexpr int kNzThreads = 256;
 constexpr int kNzWarps = kNzThreads / 32;
-constexpr int kNzItems = 16;
-constexpr int kNzTile = kNzThreads * kNzItems;  // 4096 elements per CTA
+constexpr int kNzTile = kNzThreads * 16;  // the smallest tile (SpMV): workspace sizing
+constexpr int kNzStageCap = 4096 + 2;      // row starts staged in shared memory per tile
 
 template <typename T>
 __device__ __forceinline__ float elem_f32(const T* p);
@@ -74,11 +74,11 @@ struct NzCarry {
 // non-decreasing; any bounds keep every access in range).
 template <typename IT>
 __global__ void __launch_bounds__(256) nz_rowrange_kernel(const IT* __restrict__ bounds, int64_t nseg, int64_t n,
-                                                          int64_t tiles, long long* __restrict__ row_lo) {
+                                                          int64_t tiles, int tile, long long* __restrict__ row_lo) {
   const int lane = threadIdx.x & 31;
   const int64_t t = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (t >= tiles) return;  // warp-uniform
-  const int64_t key = t * kNzTile;
+  const int64_t key = t * tile;
   int64_t lo = 0, hi = nseg + 1;  // answer in [lo, hi]: row_start(lo) <= key
   while (hi - lo > 31) {
     const int64_t step = (hi - lo + 31) / 32;
@@ -131,134 +131,136 @@ __device__ __forceinline__ ACC block_seg_scan(ACC v, int reset, ACC* sv, int* sr
 // VT: element type; ACC: accumulator / output type; SPMV: element i is
 // vals[i] * x[cols[i]] (FP32 product), else vals[i].  Segment r covers
 // [bounds[r], bounds[r + 1]) (clamped); the tiles cover all n elements.
-template <typename VT, typename ACC, bool SPMV, typename IT>
-__global__ void __launch_bounds__(kNzThreads) nz_split_kernel(const VT* __restrict__ vals,
+template <typename VT, typename ACC, bool SPMV, typename IT, int ITEMS>
+__global__ void __launch_bounds__(kNzThreads, 4) nz_split_kernel(const VT* __restrict__ vals,
                                                               const int32_t* __restrict__ cols,
                                                               const VT* __restrict__ x, int64_t x_len,
                                                               const IT* __restrict__ bounds, int64_t nseg, int64_t n,
                                                               const long long* __restrict__ row_lo,
                                                               ACC* __restrict__ out, NzCarry<ACC>* __restrict__ carry,
                                                               WsHeader* ws) {
+  constexpr int TILE = kNzThreads * ITEMS;
   __shared__ ACC sv[kNzWarps];
   __shared__ int sr[kNzWarps];
   const int64_t c = blockIdx.x;
-  const int64_t t_lo = c * kNzTile;
-  const int64_t t_hi = t_lo + kNzTile < n ? t_lo + kNzTile : n;
-  const int64_t j0 = t_lo + (int64_t)threadIdx.x * kNzItems;
-  const int64_t j_end = j0 + kNzItems < t_hi ? j0 + kNzItems : t_hi;  // this thread's [j0, j_end)
+  const int64_t t_lo = c * TILE;
+  const int64_t t_hi = t_lo + TILE < n ? t_lo + TILE : n;
+  const int64_t j0 = t_lo + (int64_t)threadIdx.x * ITEMS;
+  const int64_t j_end = j0 + ITEMS < t_hi ? j0 + ITEMS : t_hi;  // this thread's [j0, j_end)
   const bool has_items = j0 < t_hi;
   const int64_t r_tile = row_lo[c];
   const int64_t r_last = c + 1 < gridDim.x ? row_lo[c + 1] : nseg + 1;  // rows of this tile lie in [r_tile, r_last]
 
-  // ---- the thread's elements (products) ----
-  ACC p[kNzItems];
-  {
-    const bool full = j0 + kNzItems <= t_hi;
-    const bool vec_v = full && ((reinterpret_cast<uintptr_t>(vals + j0) & 15u) == 0);
-    if constexpr (SPMV) {
-      int32_t cc[kNzItems];
-      float va[kNzItems];
-      if (full && ((reinterpret_cast<uintptr_t>(cols + j0) & 15u) == 0)) {
+  // ---- the thread's elements: SpMV products, or the packed input words ----
+  const bool full = j0 + ITEMS <= t_hi;
+  const bool vec_v = full && ((reinterpret_cast<uintptr_t>(vals + j0) & 15u) == 0);
+  constexpr int WORDS = SPMV ? 1 : ITEMS * (int)sizeof(VT) / 4;
+  float p[SPMV ? ITEMS : 1];
+  uint32_t raw[WORDS];
+  if constexpr (SPMV) {
+    int32_t cc[ITEMS];
+    float va[ITEMS];
+    if (full && ((reinterpret_cast<uintptr_t>(cols + j0) & 15u) == 0)) {
 #pragma unroll
-        for (int q = 0; q < kNzItems / 4; ++q) {
-          const int4 v4 = __ldg(reinterpret_cast<const int4*>(cols + j0) + q);
-          cc[4 * q] = v4.x;
-          cc[4 * q + 1] = v4.y;
-          cc[4 * q + 2] = v4.z;
-          cc[4 * q + 3] = v4.w;
-        }
-      } else {
-#pragma unroll
-        for (int i = 0; i < kNzItems; ++i) cc[i] = j0 + i < t_hi ? __ldg(cols + j0 + i) : 0;
-      }
-      if (vec_v && sizeof(VT) == 4) {
-#pragma unroll
-        for (int q = 0; q < kNzItems / 4; ++q) {
-          const float4 v4 = __ldg(reinterpret_cast<const float4*>(vals + j0) + q);
-          va[4 * q] = v4.x;
-          va[4 * q + 1] = v4.y;
-          va[4 * q + 2] = v4.z;
-          va[4 * q + 3] = v4.w;
-        }
-      } else if (vec_v) {
-#pragma unroll
-        for (int q = 0; q < kNzItems / 8; ++q) {
-          const uint4 u = __ldg(reinterpret_cast<const uint4*>(vals + j0) + q);
-          const __half2* h = reinterpret_cast<const __half2*>(&u);
-#pragma unroll
-          for (int k = 0; k < 4; ++k) {
-            const float2 f = __half22float2(h[k]);
-            va[8 * q + 2 * k] = f.x;
-            va[8 * q + 2 * k + 1] = f.y;
-          }
-        }
-      } else {
-#pragma unroll
-        for (int i = 0; i < kNzItems; ++i) va[i] = j0 + i < t_hi ? elem_f32<VT>(vals + j0 + i) : 0.f;
-      }
-#pragma unroll
-      for (int i = 0; i < kNzItems; ++i) {
-        float xv = 0.f;
-        if ((unsigned long long)(unsigned)cc[i] < (unsigned long long)x_len) xv = elem_f32<VT>(x + cc[i]);
-        else if (j0 + i < t_hi && ws) record_error(ws, TCU_ERR_ARG, 301, (uint32_t)(j0 + i));
-        p[i] = __fmul_rn(va[i], xv);
-      }
-    } else if constexpr (sizeof(VT) == 1) {
-      if (vec_v) {
-        const uint4 u = __ldg(reinterpret_cast<const uint4*>(vals + j0));
-        const int8_t* b8 = reinterpret_cast<const int8_t*>(&u);
-#pragma unroll
-        for (int i = 0; i < kNzItems; ++i) p[i] = (ACC)b8[i];
-      } else {
-#pragma unroll
-        for (int i = 0; i < kNzItems; ++i) p[i] = j0 + i < t_hi ? (ACC)__ldg(vals + j0 + i) : (ACC)0;
+      for (int q = 0; q < ITEMS / 4; ++q) {
+        const int4 v4 = __ldg(reinterpret_cast<const int4*>(cols + j0) + q);
+        cc[4 * q] = v4.x;
+        cc[4 * q + 1] = v4.y;
+        cc[4 * q + 2] = v4.z;
+        cc[4 * q + 3] = v4.w;
       }
     } else {
-      if (vec_v && sizeof(VT) == 4) {
 #pragma unroll
-        for (int q = 0; q < kNzItems / 4; ++q) {
-          const float4 v4 = __ldg(reinterpret_cast<const float4*>(vals + j0) + q);
-          p[4 * q] = v4.x;
-          p[4 * q + 1] = v4.y;
-          p[4 * q + 2] = v4.z;
-          p[4 * q + 3] = v4.w;
+      for (int i = 0; i < ITEMS; ++i) cc[i] = j0 + i < t_hi ? __ldg(cols + j0 + i) : 0;
+    }
+    if (vec_v && sizeof(VT) == 4) {
+#pragma unroll
+      for (int q = 0; q < ITEMS / 4; ++q) {
+        const float4 v4 = __ldg(reinterpret_cast<const float4*>(vals + j0) + q);
+        va[4 * q] = v4.x;
+        va[4 * q + 1] = v4.y;
+        va[4 * q + 2] = v4.z;
+        va[4 * q + 3] = v4.w;
+      }
+    } else if (vec_v) {
+#pragma unroll
+      for (int q = 0; q < ITEMS / 8; ++q) {
+        const uint4 u = __ldg(reinterpret_cast<const uint4*>(vals + j0) + q);
+        const __half2* h = reinterpret_cast<const __half2*>(&u);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const float2 f = __half22float2(h[k]);
+          va[8 * q + 2 * k] = f.x;
+          va[8 * q + 2 * k + 1] = f.y;
         }
-      } else if (vec_v) {
+      }
+    } else {
 #pragma unroll
-        for (int q = 0; q < kNzItems / 8; ++q) {
-          const uint4 u = __ldg(reinterpret_cast<const uint4*>(vals + j0) + q);
-          const __half2* h = reinterpret_cast<const __half2*>(&u);
+      for (int i = 0; i < ITEMS; ++i) va[i] = j0 + i < t_hi ? elem_f32<VT>(vals + j0 + i) : 0.f;
+    }
 #pragma unroll
-          for (int k = 0; k < 4; ++k) {
-            const float2 f = __half22float2(h[k]);
-            p[8 * q + 2 * k] = f.x;
-            p[8 * q + 2 * k + 1] = f.y;
-          }
+    for (int i = 0; i < ITEMS; ++i) {
+      float xv = 0.f;
+      if ((unsigned long long)(unsigned)cc[i] < (unsigned long long)x_len) xv = elem_f32<VT>(x + cc[i]);
+      else if (j0 + i < t_hi && ws) record_error(ws, TCU_ERR_ARG, 301, (uint32_t)(j0 + i));
+      p[i] = __fmul_rn(va[i], xv);
+    }
+  } else {
+    if (vec_v) {
+#pragma unroll
+      for (int q = 0; q < WORDS / 4; ++q) {
+        const uint4 u = __ldg(reinterpret_cast<const uint4*>(vals + j0) + q);
+        raw[4 * q] = u.x;
+        raw[4 * q + 1] = u.y;
+        raw[4 * q + 2] = u.z;
+        raw[4 * q + 3] = u.w;
+      }
+    } else {  // ragged or unaligned: element by element, packed the same way
+#pragma unroll
+      for (int w = 0; w < WORDS; ++w) raw[w] = 0;
+      const uint8_t* vb = reinterpret_cast<const uint8_t*>(vals + j0);
+#pragma unroll
+      for (int i = 0; i < ITEMS; ++i) {
+        if (j0 + i < t_hi) {
+          uint32_t bits;
+          if constexpr (sizeof(VT) == 1) bits = vb[i];
+          else if constexpr (sizeof(VT) == 2) bits = reinterpret_cast<const uint16_t*>(vb)[i];
+          else bits = reinterpret_cast<const uint32_t*>(vb)[i];
+          raw[i * (int)sizeof(VT) / 4] |= bits << (8 * ((i * (int)sizeof(VT)) & 3));
         }
-      } else {
-#pragma unroll
-        for (int i = 0; i < kNzItems; ++i) p[i] = j0 + i < t_hi ? (ACC)elem_f32<VT>(vals + j0 + i) : (ACC)0;
       }
     }
   }
+  // element i of the thread as ACC (constant i after unrolling)
+  auto elem = [&](int i) -> ACC {
+    if constexpr (SPMV) {
+      return p[i];
+    } else if constexpr (sizeof(VT) == 1) {
+      return (ACC)(int8_t)(raw[i >> 2] >> (8 * (i & 3)));
+    } else if constexpr (sizeof(VT) == 2) {
+      return (ACC)__half2float(__ushort_as_half((unsigned short)(raw[i >> 1] >> (16 * (i & 1)))));
+    } else {
+      return (ACC)__uint_as_float(raw[i]);
+    }
+  };
 
   // ---- the starts of the tile's rows [r_tile, r_last + 1], relative to the
   // tile start and clamped to [-1, kNzTile + 1], staged in shared memory ----
-  __shared__ int s_st[kNzTile + 2];
+  __shared__ int s_st[kNzStageCap];
   const int64_t cnt = r_last - r_tile + 2;
-  const bool staged = cnt <= kNzTile + 2;  // block-uniform; else read from global memory
+  const bool staged = cnt <= kNzStageCap;  // block-uniform; else read from global memory
   if (staged) {
     for (int i = threadIdx.x; i < (int)cnt; i += kNzThreads) {
       const int64_t v = row_start(bounds, r_tile + i, nseg, n) - t_lo;
-      s_st[i] = v < -1 ? -1 : (v > kNzTile ? kNzTile + 1 : (int)v);
+      s_st[i] = v < -1 ? -1 : (v > TILE ? TILE + 1 : (int)v);
     }
   }
   __syncthreads();
   auto S = [&](int64_t ri) -> int {
     const int64_t k = ri - r_tile;
-    if (staged) return k < 0 ? -1 : (k < cnt ? s_st[k] : kNzTile + 1);
+    if (staged) return k < 0 ? -1 : (k < cnt ? s_st[k] : TILE + 1);
     const int64_t v = row_start(bounds, ri, nseg, n) - t_lo;
-    return v < -1 ? -1 : (v > kNzTile ? kNzTile + 1 : (int)v);
+    return v < -1 ? -1 : (v > TILE ? TILE + 1 : (int)v);
   };
   const int j0r = (int)(j0 - t_lo), j_endr = (int)(j_end - t_lo);  // tile-relative
 
@@ -283,7 +285,7 @@ __global__ void __launch_bounds__(kNzThreads) nz_split_kernel(const VT* __restri
   int next = has_items ? S(row + 1) : 0;
   if (has_items) {
 #pragma unroll
-    for (int i = 0; i < kNzItems; ++i) {
+    for (int i = 0; i < ITEMS; ++i) {
       const int j = j0r + i;
       if (j < j_endr) {
         while (next <= j) {  // the current row ends before element j (empty rows pass through)
@@ -298,7 +300,7 @@ __global__ void __launch_bounds__(kNzThreads) nz_split_kernel(const VT* __restri
           ++row;
           next = S(row + 1);
         }
-        acc += p[i];
+        acc += elem(i);
       }
     }
   }
@@ -326,7 +328,7 @@ __global__ void __launch_bounds__(kNzThreads) nz_split_kernel(const VT* __restri
   if ((threadIdx.x & 31) == 31) s_last[threadIdx.x >> 5] = scanned;
   __syncthreads();
   const ACC prev = (threadIdx.x & 31) ? carry_in : (threadIdx.x ? s_last[(threadIdx.x >> 5) - 1] : (ACC)0);
-  const int t_last = (int)((t_hi - t_lo - 1) / kNzItems);
+  const int t_last = (int)((t_hi - t_lo - 1) / ITEMS);
   if (threadIdx.x == 0) {
     carry[c].head_row = -1;
     carry[c].span = 0;
@@ -379,7 +381,11 @@ static tcu_status_t nz_run(const VT* vals, const int32_t* cols, const VT* x, int
   cudaError_t e = cudaMemsetAsync(out, 0, (size_t)nseg * sizeof(ACC), st);  // empty rows
   if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(row sums)");
   if (n == 0) return TCU_OK;
-  const int64_t tiles = (n + kNzTile - 1) / kNzTile;
+  // 16 elements per thread (64 per thread for sums -- 4x fewer tiles -- was
+  // measured no faster at 2^28 and slower for short segments)
+  constexpr int ITEMS = 16;
+  constexpr int TILE = kNzThreads * ITEMS;
+  const int64_t tiles = (n + TILE - 1) / TILE;
   if (tiles > 0x7FFFFFFF) return TCU_ERR_ARG;
   const size_t need = nz_scratch_bytes(tiles);
   if (!ws || ws_capacity(ws_bytes) * 16 < (int64_t)need) return TCU_ERR_WORKSPACE;
@@ -387,9 +393,9 @@ static tcu_status_t nz_run(const VT* vals, const int32_t* cols, const VT* x, int
   NzCarry<ACC>* carry = reinterpret_cast<NzCarry<ACC>*>(
       (reinterpret_cast<uintptr_t>(row_lo + tiles + 1) + 63) & ~(uintptr_t)63);
   WsHeader* h = static_cast<WsHeader*>(ws);
-  nz_rowrange_kernel<IT><<<(unsigned)((tiles * 32 + 255) / 256), 256, 0, st>>>(bounds, nseg, n, tiles, row_lo);
-  nz_split_kernel<VT, ACC, SPMV, IT><<<(unsigned)tiles, kNzThreads, 0, st>>>(vals, cols, x, x_len, bounds, nseg, n,
-                                                                             row_lo, out, carry, h);
+  nz_rowrange_kernel<IT><<<(unsigned)((tiles * 32 + 255) / 256), 256, 0, st>>>(bounds, nseg, n, tiles, TILE, row_lo);
+  nz_split_kernel<VT, ACC, SPMV, IT, ITEMS><<<(unsigned)tiles, kNzThreads, 0, st>>>(vals, cols, x, x_len, bounds, nseg,
+                                                                                    n, row_lo, out, carry, h);
   nz_fixup_kernel<ACC><<<(unsigned)((tiles + 255) / 256), 256, 0, st>>>(carry, tiles, nseg, out);
   e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "nz_split launch");
