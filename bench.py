@@ -80,7 +80,7 @@ class ClockSampler:
 
     def start(self):
         try:
-            cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100"]
+            cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "20"]
             if self.bus_id:
                 cmd += ["-i", self.bus_id]
             self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
@@ -95,6 +95,16 @@ class ClockSampler:
             parts = [s.strip() for s in line.split(",")]
             if len(parts) >= 9:
                 self.samples.append((time.time(), parts))
+
+    def wait_for(self, t, timeout=3.0):
+        """Wait (bounded) until a sample taken at or after wall time t arrives:
+        nvidia-smi needs about a second before its first line."""
+        end = time.time() + timeout
+        while time.time() < end and self.proc is not None:
+            if self.samples and self.samples[-1][0] >= t:
+                return True
+            time.sleep(0.01)
+        return False
 
     def stop(self):
         if self.proc is not None:
@@ -737,7 +747,7 @@ def main():
         bus = f"{getattr(props, 'pci_domain_id', 0):08X}:{props.pci_bus_id:02X}:{props.pci_device_id:02X}.0"
     sampler = ClockSampler(bus)
     sampler.start()
-    time.sleep(0.3)
+    sampler.wait_for(time.time(), timeout=5.0)  # sampling has started before the timed region
 
     stream = torch.cuda.current_stream(dev)
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
@@ -759,6 +769,7 @@ def main():
     total_ms = t_all0.elapsed_time(t_all1)
     per = [a.elapsed_time(b) for a, b in evs]
     tcuscan_ops.raise_device_error(dev)
+    sampler.wait_for(wall1, timeout=2.0)  # a sample after the region closes the window
     clocks = sampler.summary(wall0, wall1)
     sampler.stop()
 
