@@ -755,7 +755,7 @@ static tcu_status_t topk_t(const uint16_t* x, int64_t n, int64_t k, uint16_t* ou
   cudaError_t e = cudaMemsetAsync(tmp, 0, 2048 + sizeof(TopkState), st);
   if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(topk state)");
   const int g = rs_grid(T, 8);
-  const int gh = rs_grid(T, 3);  // histogram CTAs hold 64 KB of counters
+  const int gh = rs_grid(T, 6);  // histogram CTAs: contiguous chunks of tiles, 32 KB of counters
   if (VEC) {
     topk_hist_kernel<CODEC, 0, true><<<gh, kRsThreads, 0, st>>>(x, n, T, state, bins);
     topk_pick_kernel<0><<<1, kRsThreads, 0, st>>>(bins, k, state);
