@@ -811,6 +811,30 @@ def main():
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1)
     e2e_ms = max_over_ranks(e2e_ms, world, dev)
+    # the copy-only bound of the same step: both copies of the whole arrays,
+    # concurrently on two streams, no scan
+    s_in, s_out = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+    zd = scanner.z
+
+    def copies():
+        s_in.wait_stream(stream)
+        s_out.wait_stream(stream)
+        with torch.cuda.stream(s_in):
+            x.copy_(x_host, non_blocking=True)
+        with torch.cuda.stream(s_out):
+            z_host.copy_(zd[:n], non_blocking=True)
+        stream.wait_stream(s_in)
+        stream.wait_stream(s_out)
+
+    copies()
+    torch.cuda.synchronize()
+    c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    c0.record(stream)
+    for _ in range(3):
+        copies()
+    c1.record(stream)
+    torch.cuda.synchronize()
+    copy_ms = max_over_ranks(c0.elapsed_time(c1) / 3, world, dev)
 
     extras = None
     if rank == 0 and world == 1 and not args.no_extras:
@@ -859,7 +883,9 @@ def main():
         "cpu_baseline": cpu_base,
         "e2e": {"value": replica_throughput(world, n, e2e_steps, e2e_ms), "unit": "elem/s",
                 "h2d_bytes_per_step": n * x.element_size(), "d2h_bytes_per_step": n * 4,
-                "ms_per_step": e2e_ms / e2e_steps},
+                "ms_per_step": e2e_ms / e2e_steps,
+                # the same bytes copied with no scan (both directions at once): the PCIe bound
+                "copy_only_ms_per_step": copy_ms, "frac_of_copy_bound": copy_ms / (e2e_ms / e2e_steps)},
         "clocks": clocks,
         "gpu_launches": args.steps,
         "median_ms_per_launch": statistics.median(per),
