@@ -9,8 +9,9 @@
 // (no tensor-core reshaping).  Three launches, each a pure stream with no
 // waiting between CTAs:
 //   cmp_count_kernel    selected elements per tile (reads the mask once);
-//   cmp_offsets_kernel  one CTA: exclusive int64 scan of the tile counts ->
-//                       each tile's output offset, and the total;
+//   cmp_offsets_*       exclusive int64 scan of the tile counts in two
+//                       parallel passes (per 1024 tiles, then the block
+//                       bases) -> each tile's output offset, and the total;
 //   compress_kernel     one persistent CTA per SM, tiles assigned statically.
 //               warp 0 loads each tile's mask, values (and gathered indices)
 //               with 2-D TMA copies into a ring of shared-memory stages.  Each
@@ -364,57 +365,39 @@ __global__ void __launch_bounds__(kCmpThreads, 1)
   }
 }
 
-// Selected elements of every tile (mask != 0).  One 256-thread CTA per tile
-// at a time, grid-stride over tiles.
+// Selected elements of every tile (mask != 0): one warp per tile, every lane
+// with all of its 16-byte mask vectors in flight, a warp sum and no block
+// barrier; grid-stride over tiles.
 template <int TILE>
 __global__ void __launch_bounds__(256) cmp_count_kernel(const int8_t* __restrict__ mask, int64_t n, int64_t num_tiles,
                                                         int* __restrict__ counts) {
-  constexpr int PER = TILE / 256;  // mask bytes per thread: 8, 16 or 32
-  __shared__ int s_w[8];
-  for (int64_t t = blockIdx.x; t < num_tiles; t += gridDim.x) {
-    const int64_t e = t * TILE + (int64_t)threadIdx.x * PER;
+  constexpr int NV = TILE / 512;  // 16-byte vectors per lane: 16, 8 or 4
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * 8;
+  for (int64_t t = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5); t < num_tiles; t += warps) {  // warp-uniform
+    const int64_t e0 = t * TILE;
     int c = 0;
-    if (e + PER <= n) {
-      if constexpr (PER >= 16) {
-        const uint4* mv = reinterpret_cast<const uint4*>(mask + e);
+    if (e0 + TILE <= n) {
+      uint4 m[NV];
 #pragma unroll
-        for (int v = 0; v < PER / 16; ++v) {
-          const uint4 m = __ldg(mv + v);
-          c += __popc(sel4(m.x) | (sel4(m.y) << 4) | (sel4(m.z) << 8) | (sel4(m.w) << 12));
-        }
-      } else {
-        const uint2 m = __ldg(reinterpret_cast<const uint2*>(mask + e));
-        c += __popc(sel4(m.x) | (sel4(m.y) << 4));
-      }
+      for (int v = 0; v < NV; ++v) m[v] = __ldg(reinterpret_cast<const uint4*>(mask + e0) + v * 32 + lane);
+#pragma unroll
+      for (int v = 0; v < NV; ++v)
+        c += __popc(sel4(m[v].x) | (sel4(m[v].y) << 4) | (sel4(m[v].z) << 8) | (sel4(m[v].w) << 12));
     } else {
-      for (int j = 0; j < PER; ++j)
-        if (e + j < n) c += mask[e + j] != 0;
+      for (int64_t e = e0 + lane; e < n; e += 32) c += mask[e] != 0;
     }
     c = warp_sum_any(c);
-    if ((threadIdx.x & 31) == 0) s_w[threadIdx.x >> 5] = c;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      int tot = 0;
-#pragma unroll
-      for (int k = 0; k < 8; ++k) tot += s_w[k];
-      counts[t] = tot;
-    }
-    __syncthreads();
+    if (lane == 0) counts[t] = c;
   }
 }
 
-// Exclusive scan of the tile counts in one CTA: offsets[t] = selected before
-// tile t, offsets[num_tiles] = total, also written to *count_out.
-__global__ void __launch_bounds__(1024) cmp_offsets_kernel(const int* __restrict__ counts, int64_t num_tiles,
-                                                           long long* __restrict__ offsets, long long* count_out) {
-  __shared__ long long s_w[32];
-  const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
-  const int64_t per = (num_tiles + 1023) / 1024;
-  const int64_t b0 = (int64_t)t * per;
-  const int64_t b1 = b0 + per < num_tiles ? b0 + per : num_tiles;
-  long long sum = 0;
-  for (int64_t i = b0; i < b1; ++i) sum += counts[i];
-  long long inc = sum;
+// Tile offsets in two parallel passes.  Pass 1, one CTA per 1024 tiles:
+// exclusive scan of the counts -> offsets relative to the block, and the
+// block's total in blk[b].
+__device__ __forceinline__ long long block_excl_scan1024(long long v, long long* s_w, long long* total) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  long long inc = v;
 #pragma unroll
   for (int d = 1; d < 32; d <<= 1) {
     const long long o = __shfl_up_sync(0xffffffffu, inc, d);
@@ -423,23 +406,47 @@ __global__ void __launch_bounds__(1024) cmp_offsets_kernel(const int* __restrict
   if (lane == 31) s_w[wid] = inc;
   __syncthreads();
   if (wid == 0) {
-    long long v = s_w[lane];
+    long long w = s_w[lane];
 #pragma unroll
     for (int d = 1; d < 32; d <<= 1) {
-      const long long o = __shfl_up_sync(0xffffffffu, v, d);
-      if (lane >= d) v += o;
+      const long long o = __shfl_up_sync(0xffffffffu, w, d);
+      if (lane >= d) w += o;
     }
-    s_w[lane] = v;  // inclusive warp totals
+    s_w[lane] = w;  // inclusive warp totals
   }
   __syncthreads();
-  long long run = (wid ? s_w[wid - 1] : 0) + inc - sum;
-  for (int64_t i = b0; i < b1; ++i) {
-    offsets[i] = run;
-    run += counts[i];
-  }
-  if (t == 1023) {
-    offsets[num_tiles] = s_w[31];
-    if (count_out) *count_out = s_w[31];
+  *total = s_w[31];
+  return (wid ? s_w[wid - 1] : 0) + inc - v;
+}
+
+__global__ void __launch_bounds__(1024) cmp_offsets_local_kernel(const int* __restrict__ counts, int64_t num_tiles,
+                                                                 long long* __restrict__ offsets,
+                                                                 long long* __restrict__ blk) {
+  __shared__ long long s_w[32];
+  const int64_t t = (int64_t)blockIdx.x * 1024 + threadIdx.x;
+  const long long v = t < num_tiles ? counts[t] : 0;
+  long long tot;
+  const long long ex = block_excl_scan1024(v, s_w, &tot);
+  if (t < num_tiles) offsets[t] = ex;
+  if (threadIdx.x == 0) blk[blockIdx.x] = tot;
+}
+
+// Pass 2: each block adds the totals of the blocks before it; the last block
+// writes offsets[num_tiles] = total (and *count_out).
+__global__ void __launch_bounds__(1024) cmp_offsets_add_kernel(long long* __restrict__ offsets, int64_t num_tiles,
+                                                               const long long* __restrict__ blk, int64_t nblk,
+                                                               long long* count_out) {
+  __shared__ long long s_w[32];
+  long long part = 0;
+  for (int64_t i = threadIdx.x; i < (int64_t)blockIdx.x; i += 1024) part += blk[i];
+  long long base;
+  block_excl_scan1024(part, s_w, &base);  // only the total is used
+  const int64_t t = (int64_t)blockIdx.x * 1024 + threadIdx.x;
+  if (t < num_tiles) offsets[t] += base;
+  if (blockIdx.x == nblk - 1 && threadIdx.x == 0) {
+    const long long total = base + blk[blockIdx.x];
+    offsets[num_tiles] = total;
+    if (count_out) *count_out = total;
   }
 }
 
@@ -498,7 +505,8 @@ __global__ void __launch_bounds__(256) mask_count_kernel(const int8_t* mask, int
 // ---------------------------------------------------------------------------
 // Host side.  The tile is a function of the element and index sizes; the
 // per-tile counts and offsets sit in the workspace's descriptor region:
-// offsets[num_tiles + 1] (int64) then counts[num_tiles] (int32).
+// offsets[num_tiles + 1] (int64), counts[num_tiles] (int32), then one int64
+// block total per 1024 tiles.
 static int64_t compress_tile(int elem_bytes, int idx_bytes) { return 128 * cmp_ept(elem_bytes, idx_bytes); }
 
 static int idx_stage_bytes(int idx_mode, int idx_bytes) { return idx_mode ? idx_bytes : 0; }
@@ -506,16 +514,23 @@ static int idx_stage_bytes(int idx_mode, int idx_bytes) { return idx_mode ? idx_
 struct CmpScratch {
   long long* offsets;
   int* counts;
+  long long* blk;  // per 1024 tiles: the block total of the offset scan
   int64_t tiles;
+  int64_t nblk;
   size_t bytes;
 };
 
 static tcu_status_t cmp_scratch(void* ws, size_t ws_bytes, int64_t n, int64_t tile, CmpScratch* sc) {
   sc->tiles = (n + tile - 1) / tile;
-  sc->bytes = (size_t)(sc->tiles + 1) * 8 + (size_t)sc->tiles * 4;
-  if (!ws || ws_bytes < 128 + sc->bytes || ws_capacity(ws_bytes) < sc->tiles) return TCU_ERR_WORKSPACE;
-  sc->offsets = reinterpret_cast<long long*>(ws_descs(ws));
-  sc->counts = reinterpret_cast<int*>(sc->offsets + sc->tiles + 1);
+  sc->nblk = (sc->tiles + 1023) / 1024;
+  const size_t cnt_off = (size_t)(sc->tiles + 1) * 8;
+  const size_t blk_off = (cnt_off + (size_t)sc->tiles * 4 + 7) & ~(size_t)7;
+  sc->bytes = blk_off + (size_t)sc->nblk * 8;
+  if (!ws || ws_bytes < 128 + sc->bytes || ws_capacity(ws_bytes) * 16 < (int64_t)sc->bytes) return TCU_ERR_WORKSPACE;
+  uint8_t* base = reinterpret_cast<uint8_t*>(ws_descs(ws));
+  sc->offsets = reinterpret_cast<long long*>(base);
+  sc->counts = reinterpret_cast<int*>(base + cnt_off);
+  sc->blk = reinterpret_cast<long long*>(base + blk_off);
   return TCU_OK;
 }
 
@@ -526,13 +541,15 @@ static tcu_status_t cmp_clear(void* ws, const CmpScratch& sc, cudaStream_t st) {
 
 static tcu_status_t cmp_count(const int8_t* mask, int64_t n, int64_t tile, const CmpScratch& sc, long long* count_out,
                               cudaStream_t st) {
-  int64_t grid = sc.tiles;
+  int64_t grid = (sc.tiles + 7) / 8;  // one warp per tile
   const int64_t cap = (int64_t)sm_count() * 8;
   if (grid > cap) grid = cap;
   if (tile == 8192) cmp_count_kernel<8192><<<(int)grid, 256, 0, st>>>(mask, n, sc.tiles, sc.counts);
   else if (tile == 4096) cmp_count_kernel<4096><<<(int)grid, 256, 0, st>>>(mask, n, sc.tiles, sc.counts);
   else cmp_count_kernel<2048><<<(int)grid, 256, 0, st>>>(mask, n, sc.tiles, sc.counts);
-  cmp_offsets_kernel<<<1, 1024, 0, st>>>(sc.counts, sc.tiles, sc.offsets, count_out);
+  if (sc.nblk > 0x7FFFFFFF) return TCU_ERR_ARG;
+  cmp_offsets_local_kernel<<<(unsigned)sc.nblk, 1024, 0, st>>>(sc.counts, sc.tiles, sc.offsets, sc.blk);
+  cmp_offsets_add_kernel<<<(unsigned)sc.nblk, 1024, 0, st>>>(sc.offsets, sc.tiles, sc.blk, sc.nblk, count_out);
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? TCU_OK : cuda_fail(e, "compress count launch");
 }
