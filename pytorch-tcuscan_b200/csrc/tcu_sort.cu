@@ -479,35 +479,34 @@ __global__ void __launch_bounds__(kRsThreads) topk_pick_kernel(const unsigned* _
   }
 }
 
-// Per tile: elements above thr and equal to thr.
+// Per tile: elements above thr and equal to thr -- one warp per tile (each
+// lane 128 consecutive elements in 16-byte loads, all in flight), a warp sum,
+// no block barrier.
 template <int CODEC, bool VEC>
 __global__ void __launch_bounds__(kRsThreads) topk_count_kernel(const uint16_t* __restrict__ x, int64_t n,
                                                                 int64_t num_tiles, const TopkState* __restrict__ st,
                                                                 int* __restrict__ c_above, int* __restrict__ c_tie) {
-  __shared__ int s_c[2][kRsWarps];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
   const uint32_t thr = (uint32_t)st->thr;
-  int par = 0;
-  for (int64_t t = blockIdx.x; t < num_tiles; t += gridDim.x, par ^= 1) {
-    const int64_t e0 = t * kRsTile + (int64_t)threadIdx.x * kRsEpt;
-    uint16_t v[16];
-    load16<VEC>(x, e0, n, v);
+  const int64_t warps = (int64_t)gridDim.x * kRsWarps;
+  for (int64_t t = (int64_t)blockIdx.x * kRsWarps + (threadIdx.x >> 5); t < num_tiles; t += warps) {  // warp-uniform
     int aq = 0;  // above in the low half, equal in the high half
 #pragma unroll
-    for (int j = 0; j < 16; ++j) {
-      const uint32_t k = topk_key<CODEC>(v[j]);
-      const bool in = e0 + j < n;
-      aq += (in && k > thr) ? 1 : ((in && k == thr) ? 0x10000 : 0);
+    for (int q = 0; q < kRsTile / 32 / 16; ++q) {  // 8 runs of 16 elements per lane
+      const int64_t e0 = t * kRsTile + ((int64_t)q * 32 + lane) * 16;
+      uint16_t v[16];
+      load16<VEC>(x, e0, n, v);
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const uint32_t k = topk_key<CODEC>(v[j]);
+        const bool in = e0 + j < n;
+        aq += (in && k > thr) ? 1 : ((in && k == thr) ? 0x10000 : 0);
+      }
     }
     aq = warp_sum_any(aq);
-    if (lane == 0) s_c[par][w] = aq;
-    __syncthreads();  // alternating slots: one barrier per tile
-    if (threadIdx.x == 0) {
-      int tot = 0;
-#pragma unroll
-      for (int k = 0; k < kRsWarps; ++k) tot += s_c[par][k];
-      c_above[t] = tot & 0xFFFF;
-      c_tie[t] = tot >> 16;
+    if (lane == 0) {
+      c_above[t] = aq & 0xFFFF;
+      c_tie[t] = aq >> 16;
     }
   }
 }
@@ -755,13 +754,14 @@ static tcu_status_t topk_t(const uint16_t* x, int64_t n, int64_t k, uint16_t* ou
   cudaError_t e = cudaMemsetAsync(tmp, 0, 2048 + sizeof(TopkState), st);
   if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(topk state)");
   const int g = rs_grid(T, 8);
+  const int gw = rs_grid((T + kRsWarps - 1) / kRsWarps, 8);  // a warp per tile
   const int gh = rs_grid(T, 6);  // histogram CTAs: contiguous chunks of tiles, 32 KB of counters
   if (VEC) {
     topk_hist_kernel<CODEC, 0, true><<<gh, kRsThreads, 0, st>>>(x, n, T, state, bins);
     topk_pick_kernel<0><<<1, kRsThreads, 0, st>>>(bins, k, state);
     topk_hist_kernel<CODEC, 1, true><<<gh, kRsThreads, 0, st>>>(x, n, T, state, bins + 256);
     topk_pick_kernel<1><<<1, kRsThreads, 0, st>>>(bins + 256, k, state);
-    topk_count_kernel<CODEC, true><<<g, kRsThreads, 0, st>>>(x, n, T, state, c_above, c_tie);
+    topk_count_kernel<CODEC, true><<<gw, kRsThreads, 0, st>>>(x, n, T, state, c_above, c_tie);
     topk_offsets_kernel<<<1, kRsThreads, 0, st>>>(c_above, c_tie, T, state, tie_before, off);
     topk_emit_kernel<CODEC, true><<<g, kRsThreads, 0, st>>>(x, n, T, state, tie_before, off, k, out, idx_out);
   } else {
@@ -769,7 +769,7 @@ static tcu_status_t topk_t(const uint16_t* x, int64_t n, int64_t k, uint16_t* ou
     topk_pick_kernel<0><<<1, kRsThreads, 0, st>>>(bins, k, state);
     topk_hist_kernel<CODEC, 1, false><<<gh, kRsThreads, 0, st>>>(x, n, T, state, bins + 256);
     topk_pick_kernel<1><<<1, kRsThreads, 0, st>>>(bins + 256, k, state);
-    topk_count_kernel<CODEC, false><<<g, kRsThreads, 0, st>>>(x, n, T, state, c_above, c_tie);
+    topk_count_kernel<CODEC, false><<<gw, kRsThreads, 0, st>>>(x, n, T, state, c_above, c_tie);
     topk_offsets_kernel<<<1, kRsThreads, 0, st>>>(c_above, c_tie, T, state, tie_before, off);
     topk_emit_kernel<CODEC, false><<<g, kRsThreads, 0, st>>>(x, n, T, state, tie_before, off, k, out, idx_out);
   }
