@@ -7,8 +7,8 @@ checkout (never copied).  Output goes to oracle/_ref/ only.  Usage:
     python oracle/build_ref.py [--ref /path/to/reference]
 
 The built module is test infrastructure: tests/golden/make_golden.py uses it to
-pin the oracle, and bench.py's CPU baseline times it.  The GPU box only loads
-the prebuilt .so (the reference checkout is not needed there).
+pin the oracle, and bench.py's CPU baseline times it.  Machines without the
+reference checkout only load the prebuilt .so.
 """
 import argparse
 import glob

@@ -1,6 +1,7 @@
 /*
  * tcu_oracle.c -- CPU restatement of the tcuscan scan family, used ONLY as
- * test infrastructure (the parity checker and the timed CPU "port" baseline).
+ * test infrastructure (the reference of the parity tests and the timed CPU
+ * "port" baseline).
  * Nothing in the product links or calls this file.
  *
  * Every function states the reference file:line whose semantics it restates.

@@ -22,8 +22,8 @@ Two sources of expected outputs, both the reference's own code:
    scipy ``B @ vector`` (test_spmv_v2.py), torch.tril (test_gen_lower.py).
 
 Inputs follow each test's own recipe (value ranges, seeds 42) at small sizes
-so the fixtures stay a few hundred KB.  The fixtures travel with the repo; the
-GPU box never needs the reference checkout.
+so the fixtures stay a few hundred KB.  The fixtures travel with the repo, so
+running the tests never needs the reference checkout.
 """
 import argparse
 import ast
