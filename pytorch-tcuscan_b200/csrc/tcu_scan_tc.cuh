@@ -229,12 +229,15 @@ __device__ __forceinline__ void split_bf16x4(const float4 v, uint2& hi, uint2& l
 // +term_bytes, same swizzle); the row is rewritten as 64 bf16 hi = RN(x) in
 // the first slot and 64 bf16 lo = RN(x - hi) in the second, the two MMA
 // operand tiles.  A row is fully read (8 lanes x 2 x 16 B) before any lane
-// writes it.  Rows in [r_lo, vrows) are also summed into acc (FP32 per lane).
+// writes it.  Rows in [r_lo, vrows) are also summed into acc: FP32 per lane
+// in two chains (at most 64 values each), the caller adds each stage's
+// partial to an FP64 aggregate.
 __device__ __forceinline__ void convert_f32_rows(uint8_t* X0, int term_bytes, int it_lo, int it_hi, int r_lo,
-                                                 int vrows, bool sums, double& acc) {
+                                                 int vrows, bool sums, float& acc) {
   uint8_t* X1 = X0 + term_bytes;
   const int lane = threadIdx.x & 31;
   const int rr = lane >> 3, cidx = lane & 7;
+  float c0 = 0.f, c1 = 0.f;
 #pragma unroll 4
   for (int it = it_lo; it < it_hi; ++it) {
     const int row = it * 4 + rr;
@@ -242,7 +245,11 @@ __device__ __forceinline__ void convert_f32_rows(uint8_t* X0, int term_bytes, in
     const float4 a = *reinterpret_cast<const float4*>(X0 + off);
     const float4 b = *reinterpret_cast<const float4*>(X1 + off);
     __syncwarp();
-    if (sums && row < vrows && row >= r_lo) acc += (double)(((a.x + a.y) + (a.z + a.w)) + ((b.x + b.y) + (b.z + b.w)));
+    if (sums && row < vrows && row >= r_lo) {
+      const float v = ((a.x + a.y) + (a.z + a.w)) + ((b.x + b.y) + (b.z + b.w));
+      if (it & 1) c1 += v;
+      else c0 += v;
+    }
     uint2 ha, la, hb, lb;
     split_bf16x4(a, ha, la);
     split_bf16x4(b, hb, lb);
@@ -252,6 +259,7 @@ __device__ __forceinline__ void convert_f32_rows(uint8_t* X0, int term_bytes, in
     *reinterpret_cast<uint2*>(X1 + swz(row * 128 + (cidx >> 1) * 16, 128) + half) = la;
     *reinterpret_cast<uint2*>(X1 + swz(row * 128 + (4 + (cidx >> 1)) * 16, 128) + half) = lb;
   }
+  acc += c0 + c1;
   fence_proxy_async_smem();  // generic-proxy writes -> tcgen05 operand reads
   __syncwarp();
 }
@@ -260,7 +268,7 @@ __device__ __forceinline__ void convert_f32_rows(uint8_t* X0, int term_bytes, in
 // pre-split stage (hi rows at X0, lo rows at X0 + term_bytes; the swizzle
 // only permutes 16-byte chunks inside a row, so rows are read as stored).
 __device__ __forceinline__ void sum_split_rows(const uint8_t* X0, int term_bytes, int it_lo, int it_hi, int r_lo,
-                                               int vrows, double& acc) {
+                                               int vrows, float& acc) {
   const int lane = threadIdx.x & 31;
   const int rr = lane >> 3, cidx = lane & 7;
 #pragma unroll 4
@@ -277,7 +285,7 @@ __device__ __forceinline__ void sum_split_rows(const uint8_t* X0, int term_bytes
         const float2 a = __bfloat1622float2(hb[t]), b = __bfloat1622float2(lb[t]);
         t8 += (a.x + b.x) + (a.y + b.y);
       }
-      acc += (double)t8;
+      acc += t8;
     }
   }
 }
@@ -714,13 +722,13 @@ __device__ __forceinline__ void scan_summer(const ScanParams& p, uint8_t* smem, 
         const int64_t row0 = ((int64_t)tid * BPT + j) * 128;
         const int64_t vr = p.full_rows - row0;
         const int vrows = vr <= 0 ? 0 : (vr >= 128 ? 128 : (int)vr);
-        double acc = 0.0;
+        float acc = 0.f;  // this stage's partial (FP32), then the FP64 tile aggregate
         if constexpr (C::PRESPLIT) {
           if (SUMS) sum_split_rows(X0, C::TERM_BYTES, 0, 16, r_lo, vrows, acc);
         } else {
           convert_f32_rows(X0, C::TERM_BYTES, 0, 16, r_lo, vrows, SUMS, acc);
         }
-        accd += acc;
+        accd += (double)acc;
         if (lane == 0) mbar_arrive(&ctl->conv[s]);
         if constexpr (SUMS) {  // the other half's sum, stored before its conv arrival
           const bool okc = __all_sync(0xffffffffu, mbar_wait(&ctl->conv[s], (k / C::NSTAGE) & 1u, wc, 9, i));
@@ -863,14 +871,14 @@ __device__ __forceinline__ void scan_converter2(const ScanParams& p, uint8_t* sm
         const int64_t row0 = ((int64_t)tid * BPT + j) * 128;
         const int64_t vr = p.full_rows - row0;
         const int vrows = vr <= 0 ? 0 : (vr >= 128 ? 128 : (int)vr);
-        double acc = 0.0;
+        float acc = 0.f;
         if constexpr (C::PRESPLIT) {
           if (SUMS) sum_split_rows(smem + s * C::STAGE_BYTES, C::TERM_BYTES, 16, 32, r_lo, vrows, acc);
         } else {
           convert_f32_rows(smem + s * C::STAGE_BYTES, C::TERM_BYTES, 16, 32, r_lo, vrows, SUMS, acc);
         }
         if constexpr (SUMS) {
-          const double t = warp_sum_any(acc);
+          const double t = warp_sum_any((double)acc);
           if (lane == 0) ctl->cv_sum[s] = t;
         }
         __syncwarp();
