@@ -421,14 +421,20 @@ __device__ __forceinline__ long long block_excl_scan1024(long long v, long long*
 
 __global__ void __launch_bounds__(1024) cmp_offsets_local_kernel(const int* __restrict__ counts, int64_t num_tiles,
                                                                  long long* __restrict__ offsets,
-                                                                 long long* __restrict__ blk) {
+                                                                 long long* __restrict__ blk, long long* count_out) {
   __shared__ long long s_w[32];
   const int64_t t = (int64_t)blockIdx.x * 1024 + threadIdx.x;
   const long long v = t < num_tiles ? counts[t] : 0;
   long long tot;
   const long long ex = block_excl_scan1024(v, s_w, &tot);
   if (t < num_tiles) offsets[t] = ex;
-  if (threadIdx.x == 0) blk[blockIdx.x] = tot;
+  if (threadIdx.x == 0) {
+    blk[blockIdx.x] = tot;
+    if (gridDim.x == 1) {  // one block: these are the final offsets (no second pass)
+      offsets[num_tiles] = tot;
+      if (count_out) *count_out = tot;
+    }
+  }
 }
 
 // Pass 2: each block adds the totals of the blocks before it; the last block
@@ -548,8 +554,9 @@ static tcu_status_t cmp_count(const int8_t* mask, int64_t n, int64_t tile, const
   else if (tile == 4096) cmp_count_kernel<4096><<<(int)grid, 256, 0, st>>>(mask, n, sc.tiles, sc.counts);
   else cmp_count_kernel<2048><<<(int)grid, 256, 0, st>>>(mask, n, sc.tiles, sc.counts);
   if (sc.nblk > 0x7FFFFFFF) return TCU_ERR_ARG;
-  cmp_offsets_local_kernel<<<(unsigned)sc.nblk, 1024, 0, st>>>(sc.counts, sc.tiles, sc.offsets, sc.blk);
-  cmp_offsets_add_kernel<<<(unsigned)sc.nblk, 1024, 0, st>>>(sc.offsets, sc.tiles, sc.blk, sc.nblk, count_out);
+  cmp_offsets_local_kernel<<<(unsigned)sc.nblk, 1024, 0, st>>>(sc.counts, sc.tiles, sc.offsets, sc.blk, count_out);
+  if (sc.nblk > 1)
+    cmp_offsets_add_kernel<<<(unsigned)sc.nblk, 1024, 0, st>>>(sc.offsets, sc.tiles, sc.blk, sc.nblk, count_out);
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? TCU_OK : cuda_fail(e, "compress count launch");
 }
