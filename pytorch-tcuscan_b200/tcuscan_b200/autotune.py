@@ -43,6 +43,7 @@ _DEFAULTS = {
 CACHE = os.environ.get("TCU_AUTOTUNE_CACHE", os.path.join(os.path.dirname(os.path.abspath(__file__)), "autotune.json"))
 _table = None
 _ctas_now = 0
+_best_cache = {}  # (op, dtype, floor(log2 n)) -> (S, ctas): lookups on every call stay cheap
 
 
 def _dname(dtype):
@@ -73,6 +74,7 @@ def reload(path=None):
     if path is not None:
         CACHE = path
     _table = None
+    _best_cache.clear()
 
 
 def best(op, dtype, n=None):
@@ -80,6 +82,16 @@ def best(op, dtype, n=None):
     default = (_DEFAULTS.get((op, dtype), 64), 0)
     if n is None:
         return default
+    ck = (op, dtype, max(int(n), 1).bit_length() - 1)
+    hit = _best_cache.get(ck)
+    if hit is not None:
+        return hit
+    r = _best_lookup(op, dtype, n, default)
+    _best_cache[ck] = r
+    return r
+
+
+def _best_lookup(op, dtype, n, default):
     tab = _load()
     if not tab:
         return default
