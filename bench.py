@@ -571,7 +571,8 @@ def run_reference_arm(args):
 
 
 PROFILE_OPS = ("compress_f16", "compress_f32", "compress_ind_f16", "spmv_f32", "spmv_f16", "serve", "segscan_i8",
-               "segscan_f16", "segsum_i8", "segsum_f16", "segsum_f32", "split_f16", "sort_f16", "topk_f16")
+               "segscan_f16", "segsum_i8", "segsum_f16", "segsum_f32", "split_f16", "sort_f16", "topk_f16",
+               "rowsum_f16")
 
 
 def run_profile_op(args, dev):
@@ -598,6 +599,24 @@ def run_profile_op(args, dev):
         else:
             fn = lambda: tcuscan_ops.run_compress_pos(xv, mask, k, 64)  # noqa: E731
             nbytes = n * (eb + 1) + k * eb
+        units = n
+    elif op == "rowsum_f16":
+        # element-split segment sums (tcu_seg_sum_rows), geometric segments of mean --seg-mean
+        xv = workloads.scan_input(n, torch.float16, dev, seed=5)
+        stp = torch.empty(n // args.seg_mean + 1024, device=dev).geometric_(1 / args.seg_mean).to(torch.int64)
+        pts = torch.cumsum(stp, 0)
+        bnd = torch.cat([torch.zeros(1, dtype=torch.int64, device=dev), pts[pts < n],
+                         torch.full((1,), n, dtype=torch.int64, device=dev)])
+        out = torch.empty(bnd.numel() - 1, dtype=torch.float32, device=dev)
+        from tcuscan_ops import _lib as L
+
+        ws, wsb = L.workspace(dev, L.lib.tcu_rows_workspace_bytes(n))
+        sp = tcuscan_ops.stream_ptr(dev)
+
+        def fn():
+            tcuscan_ops.check(L.lib.tcu_seg_sum_rows(xv.data_ptr(), L.TCU_FLOAT16, n, bnd.data_ptr(), L.TCU_INT64,
+                                                     bnd.numel(), out.data_ptr(), ws, wsb, sp), op)
+        nbytes = n * 2 + bnd.numel() * 8 + out.numel() * 4
         units = n
     elif op in ("split_f16", "sort_f16", "topk_f16"):
         xv = torch.rand(n, device=dev).half()
