@@ -244,6 +244,28 @@ __global__ void __launch_bounds__(kNzThreads, 4) nz_split_kernel(const VT* __res
     }
   };
 
+  // ---- fast path: the next tile's first element is in this tile's first row,
+  // so the whole tile lies in one row that goes on past it (block-uniform) ----
+  if (c + 1 < gridDim.x && r_tile == r_last) {
+    ACC part = (ACC)0;
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i) part += elem(i);  // every thread of this tile is full
+    part = warp_sum_any(part);
+    if ((threadIdx.x & 31) == 0) sv[threadIdx.x >> 5] = part;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      ACC tot = (ACC)0;
+#pragma unroll
+      for (int k = 0; k < kNzWarps; ++k) tot += sv[k];
+      const bool began_before = row_start(bounds, r_tile, nseg, n) < t_lo;
+      carry[c].head_row = -1;
+      carry[c].tail_row = r_tile;  // the row goes on into the next tile
+      carry[c].tail_val = tot;
+      carry[c].span = began_before ? 1 : 0;  // else the row begins here (a tail)
+    }
+    return;
+  }
+
   // ---- the starts of the tile's rows [r_tile, r_last + 1], relative to the
   // tile start and clamped to [-1, kNzTile + 1], staged in shared memory ----
   __shared__ int s_st[kNzStageCap];
