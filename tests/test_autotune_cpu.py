@@ -89,3 +89,28 @@ def test_pick_S_uses_table(at, tmp_path):
     assert tcuscan_ops._pick_S(0, torch.float16, 1 << 24, op="seg") == 32
     with pytest.raises(ValueError):
         tcuscan_ops._pick_S(48, torch.int8)
+
+
+def test_lookup_cache_cleared_on_reload(at, tmp_path):
+    p1, p2 = tmp_path / "a.json", tmp_path / "b.json"
+    p1.write_text(json.dumps({"entries": {"scan/int8/24": {"S": 32, "ctas": 0}}}))
+    p2.write_text(json.dumps({"entries": {"scan/int8/24": {"S": 64, "ctas": 0}}}))
+    at.reload(str(p1))
+    assert at.best("scan", torch.int8, 1 << 24) == (32, 0)
+    assert at.best("scan", torch.int8, (1 << 24) + 5) == (32, 0)  # same size class, cached
+    at.reload(str(p2))
+    assert at.best("scan", torch.int8, 1 << 24) == (64, 0)
+
+
+def test_segment_sum_dispatch_rule(monkeypatch):
+    import tcuscan_ops
+
+    monkeypatch.setattr(tcuscan_ops, "ROWS_MAX_MEAN", 32)
+    monkeypatch.setattr(tcuscan_ops, "ROWS_FP32", True)
+    assert tcuscan_ops._rows_for(torch.float16, 32 * 100, 100)  # mean 32: element-split
+    assert not tcuscan_ops._rows_for(torch.float16, 33 * 100, 100)  # longer: tensor cores
+    assert not tcuscan_ops._rows_for(torch.int8, 1 << 20, 16)
+    assert tcuscan_ops._rows_for(torch.float32, 1 << 20, 16)  # fp32: always element-split
+    assert not tcuscan_ops._rows_for(torch.float16, 10, 0)  # no segments
+    monkeypatch.setattr(tcuscan_ops, "ROWS_FP32", False)
+    assert not tcuscan_ops._rows_for(torch.float32, 1 << 20, 16)
