@@ -122,9 +122,11 @@ TCU_API tcu_status_t tcu_scan_chained(const void* x, tcu_dtype_t x_dtype, int64_
  * fixed 1 MiB array inside the library, held by every GPU that loads it
  * until exit; so n is limited to 2,147,221,504 elements and larger n returns
  * TCU_ERR_ARG.  The first call on a device looks the array up and zeroes it
- * on `stream`: make that first call before any stream capture.  All calls
- * share the array and it keeps the last call's contents, so calls that can
- * overlap on the GPU (other streams, other threads) race -- serialise them.
+ * on `stream`: make that first call before any stream capture.  The address
+ * is kept for the life of the process, so do not call this entry point on a
+ * device after cudaDeviceReset has been called on it.  All calls share the
+ * array and it keeps the last call's contents, so calls that can overlap on
+ * the GPU (other streams, other threads) race -- serialise them.
  * Device-side wait timeouts are not reported by this variant (tcu_scan with
  * a workspace reports them through tcu_workspace_error).                   */
 TCU_API tcu_status_t tcu_scan_noalloc(const void* x, tcu_dtype_t x_dtype, int64_t n, int S, double start, void* z,

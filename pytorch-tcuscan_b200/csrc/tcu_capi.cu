@@ -496,7 +496,8 @@ constexpr int64_t kNoAllocMaxN = (int64_t)((kNoAllocScratchBytes - 128) / sizeof
 static __device__ __align__(256) uint8_t g_noalloc_scratch[kNoAllocScratchBytes];
 
 // Device address of the scratch on the current device.  The first call on a
-// device looks the address up and zeroes the array on `st`.
+// device looks the address up and zeroes the array on `st`; the address is
+// cached for the life of the process (a cudaDeviceReset would make it stale).
 static tcu_status_t noalloc_scratch(cudaStream_t st, void** out) {
   static std::mutex mu;
   static void* ptrs[64] = {};
