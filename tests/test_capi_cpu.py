@@ -32,6 +32,64 @@ def test_library_exports_every_declared_symbol():
     assert not missing, missing
 
 
+_C_TYPES = {"tcu_status_t": ctypes.c_int, "tcu_dtype_t": ctypes.c_int, "int": ctypes.c_int,
+            "int64_t": ctypes.c_int64, "uint64_t": ctypes.c_uint64, "uint32_t": ctypes.c_uint32,
+            "size_t": ctypes.c_size_t, "double": ctypes.c_double, "void": None}
+
+
+def _header_signatures():
+    """(return type, name, [parameter types]) of every TCU_API declaration;
+    pointer and array parameters read as 'ptr'."""
+    def ctype(t):
+        t = " ".join(t.replace("const", "").split())
+        if "char" in t and "*" in t:
+            return ctypes.c_char_p
+        return "ptr" if ("*" in t or "[" in t) else _C_TYPES[t]
+
+    sigs = []
+    for h in HEADERS:
+        txt = re.sub(r"/\*.*?\*/", "", open(h).read(), flags=re.S)
+        for ret, name, params in re.findall(r"TCU_API\s+([\w\s\*]+?)\s*\b(tcu_\w+)\s*\(([^)]*)\)\s*;", txt):
+            args = []
+            for p in params.split(","):
+                p = p.strip()
+                if p in ("", "void"):
+                    continue
+                m = re.match(r"(.*?)\w+\s*(\[\d*\])?$", p)
+                args.append(ctype(m.group(1) + (m.group(2) or "")))
+            sigs.append((ctype(ret), name, args))
+    return sigs
+
+
+def test_bindings_match_header_signatures():
+    """Every signature tcuscan_ops._lib declares to ctypes agrees with the
+    header: return type, arity, and each argument's width (a 64-bit size
+    passed as a C int would be truncated silently)."""
+    import tcuscan_ops._lib as L
+
+    sigs = _header_signatures()
+    assert len(sigs) == len(_declared())
+    bound, bad = 0, []
+    for ret, name, args in sigs:
+        f = getattr(L.lib, name)
+        if f.argtypes is None:
+            continue  # not bound by the package (a test binds it itself)
+        bound += 1
+        if f.restype is not ret:
+            bad.append((name, "return", f.restype, ret))
+        if len(f.argtypes) != len(args):
+            bad.append((name, "arity", len(f.argtypes), len(args)))
+            continue
+        for i, (got, want) in enumerate(zip(f.argtypes, args)):
+            if want == "ptr":
+                ok = got is ctypes.c_void_p or (isinstance(got, type) and issubclass(got, ctypes._Pointer))
+            else:
+                ok = got is want
+            if not ok:
+                bad.append((name, i, got, want))
+    assert bound >= 40 and not bad, bad
+
+
 def test_status_strings_and_version():
     import tcuscan_ops._lib as L
 
