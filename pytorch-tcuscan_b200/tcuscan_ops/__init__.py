@@ -52,7 +52,7 @@ def _pick_S(S, dtype, n=None, op="scan"):
 def _scan_out_dtype(dtype):
     if dtype == torch.int8:
         return torch.int32
-    if dtype in (torch.float16, torch.float32, torch.bfloat16):
+    if dtype in (torch.float16, torch.float32):
         return torch.float32
     raise TypeError(f"unsupported dtype {dtype}: scans take int8, float16 or float32")
 

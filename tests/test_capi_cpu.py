@@ -133,6 +133,18 @@ def test_python_layer_rejects_cpu_tensors():
         tcuscan_ops.run_scan_multi_core(torch.zeros(10, dtype=torch.int8, device="meta"), 64)
 
 
+@pytest.mark.parametrize("dtype", [torch.bfloat16, torch.int16, torch.float64])
+def test_scan_output_dtype_rejects_unsupported_inputs(dtype):
+    """Scans and sums take int8, float16 or float32; anything else is a
+    TypeError before any launch."""
+    import tcuscan_ops
+
+    assert tcuscan_ops._scan_out_dtype(torch.int8) == torch.int32
+    assert tcuscan_ops._scan_out_dtype(torch.float16) == torch.float32
+    with pytest.raises(TypeError):
+        tcuscan_ops._scan_out_dtype(dtype)
+
+
 def test_run_scan_cpu_api():
     import tcuscan_ops
 
