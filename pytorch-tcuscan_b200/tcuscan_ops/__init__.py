@@ -543,6 +543,8 @@ def run_complete_rows(x, sums, tile_width, tile_height):
     if nb == 0 or n % nb != 0:
         raise ValueError("run_complete_rows: len(x) must be a multiple of len(sums)")
     width = int(tile_width)
+    if width <= 0:
+        raise ValueError(f"run_complete_rows: tile_width must be positive, got {width}")
     rows = (n // nb + width - 1) // width
     z = torch.empty(n, dtype=x.dtype, device=x.device)
     if n == 0:
@@ -752,7 +754,7 @@ def run_scan_batch(x, S):
     L = x.shape[-1]
     B = x.numel() // L if L else 0
     if x.dtype not in (torch.float16, torch.int8, torch.float32):
-        raise TypeError(f"run_scan_batch: x must be float16 or float32, got {x.dtype}")
+        raise TypeError(f"run_scan_batch: x must be float16, int8 or float32, got {x.dtype}")
     z = torch.empty((B, L), dtype=_scan_out_dtype(x.dtype), device=x.device)
     if B == 0 or L == 0:
         return z

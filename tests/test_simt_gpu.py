@@ -138,6 +138,14 @@ def test_complete_rows_grid(num_blocks, tile_len):
     assert oracle.max_rel_err(z, oracle.complete_rows(x.numpy(), sums.numpy(), tile_len)) < FP_TOL
 
 
+def test_complete_rows_rejects_non_positive_width():
+    import tcuscan_ops
+
+    x = torch.zeros(64, device=DEV)
+    with pytest.raises(ValueError):
+        tcuscan_ops.run_complete_rows(x, torch.zeros(2, device=DEV), 0, 0)
+
+
 def test_complete_blocks_golden(golden):
     import tcuscan_ops
 
