@@ -15,6 +15,10 @@ steps.
 
 Multi-GPU (torchrun): replicas only -- every rank scans its own array; the
 path has no exchange step, so no collective is issued (scaling = weak).
+
+Output: the other configured workloads in full detail on one JSON line
+(``{"extras": ...}``), then the headline line, which carries a compact
+``legs`` summary of the same workloads (value, time, HBM fraction, error).
 """
 import argparse
 import json
@@ -66,7 +70,7 @@ def profile_traffic(op):
 
 
 class ClockSampler:
-    """nvidia-smi clocks/throttle reasons sampled every 100 ms in the background."""
+    """nvidia-smi clocks/throttle reasons sampled every 20 ms in the background."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -193,12 +197,16 @@ def measure_extras(dev, steps=10, warmup=3):
     # compaction, 2^28, mask Bernoulli(0.3): one single-pass kernel per step
     mask = workloads.bernoulli_mask(n, 0.3, dev, seed=8)
     k = int(mask.sum().item())
+    mb = mask.bool()
     for name, dt in (("compress_f16", torch.float16), ("compress_i16", torch.int16), ("compress_f32", torch.float32)):
         xv = torch.randint(-1000, 1000, (n,), device=dev).to(dt)
         ms = _device_ms(lambda: tcuscan_ops.run_compress_pos(xv, mask, k, 64), steps, warmup)
+        exact = bool(torch.equal(tcuscan_ops.run_compress_pos(xv, mask, k, 64), torch.masked_select(xv, mb)))
         eb = xv.element_size()
-        out[name] = entry(n, n * (eb + 1) + k * eb, ms, selected=k)
+        out[name] = entry(n, n * (eb + 1) + k * eb, ms, selected=k, exact_vs_masked_select=exact,
+                          max_rel_err_vs_fp64=0.0 if exact else None)
         del xv
+    del mb
     xv = torch.randn(n, device=dev).half()
     ms = _device_ms(lambda: tcuscan_ops.run_compress_ind_no_arange(xv, mask, 64), 3, 1)
     out["compress_ind_no_arange_f16_incl_count_sync"] = entry(n, n * 3 + k * 6, ms, selected=k)
@@ -230,8 +238,17 @@ def measure_extras(dev, steps=10, warmup=3):
     xf = workloads.scan_input(n, torch.float16, dev, seed=12)
     fl = workloads.bernoulli_mask(n, 0.01, dev, seed=13)
     ms = _device_ms(lambda: tcuscan_ops.run_seg_scan(xf, fl, 64), steps, warmup)
-    out["seg_scan_flags_f16_2e28"] = entry(n, n * (2 + 1 + 4), ms)
-    del xf, fl
+    zf = tcuscan_ops.run_seg_scan(xf, fl, 64)
+    # FP64 reference: cumsum minus the cumsum just before each element's segment start
+    cs = torch.cumsum(xf.double(), 0)
+    sid = torch.cumsum(fl.long(), 0)  # segment index of every element (0 = before the first start)
+    starts = torch.nonzero(fl).flatten()
+    base = torch.cat([torch.zeros(1, dtype=torch.float64, device=dev),
+                      torch.where(starts > 0, cs[(starts - 1).clamp_min(0)], torch.zeros_like(cs[:1]))])
+    ref = cs - base[sid]
+    err = ((zf.double() - ref).abs() / ref.abs().clamp_min(1.0)).max().item()
+    out["seg_scan_flags_f16_2e28"] = entry(n, n * (2 + 1 + 4), ms, max_rel_err_vs_fp64=err)
+    del xf, fl, zf, cs, sid, starts, base, ref
 
     # CSR SpMV (products + indptr segment sums)
     for name, dt in (("spmv_f32", torch.float32), ("spmv_f16", torch.float16)):
@@ -492,6 +509,66 @@ def measure_serving(dev, count=20000, seed=11, sample=240):
     return out
 
 
+def _sig(v, digits=4):
+    """A float rounded to `digits` significant digits (compact JSON); other values unchanged."""
+    if isinstance(v, float) and v == v and v not in (float("inf"), float("-inf")) and v != 0.0:
+        return float(f"{v:.{digits}g}")
+    return v
+
+
+LEG_KEYS = ("scan_f16_2e28", "compress_f16", "compress_f32", "seg_scan_flags_f16_2e28", "spmv_f32", "spmv_f16",
+            "batch_rows_f32_4096", "scan_f16_2e20")
+
+
+def legs_summary(extras):
+    """Compact per-workload summary for the headline line: throughput, time,
+    fraction of the measured HBM peak and max relative error vs FP64 (0 for
+    exact integer / compaction results), plus the served-stream figures."""
+    if not extras:
+        return None
+    legs = {}
+    for k in LEG_KEYS:
+        e = extras.get(k)
+        if not e:
+            continue
+        d = {"value": _sig(e["value"]), "unit": e["unit"], "ms": _sig(e["ms"]), "hbm_frac": _sig(e["hbm_frac"], 3),
+             "max_rel_err": _sig(e.get("max_rel_err_vs_fp64"), 3)}
+        if "host_call_us" in e:
+            d["host_call_us"] = _sig(e["host_call_us"], 3)
+        legs[k] = d
+    sv = extras.get("served_stream")
+    if sv:
+        errs = sv.get("sample_max_rel_err_vs_fp64_served", {}) or {}
+        legs["served"] = {
+            "served_over_one_call": _sig(sv["served_over_one_call"], 3),
+            "served_req_per_s": _sig(sv["served_req_per_s"]), "one_call_req_per_s": _sig(sv["one_call_req_per_s"]),
+            "served_GB/s": _sig(sv["served_GB/s"]), "p50_ms": _sig(sv["served_p50_ms"], 3),
+            "p99_ms": _sig(sv["served_p99_ms"], 3),
+            "integer_results_identical": sv.get("sample_integer_results_identical"),
+            "max_rel_err": _sig(max(errs.values()), 3) if errs else None,
+        }
+    return legs
+
+
+def verify_headline(x, z):
+    """Checks the headline scan's output on the device outside the timed
+    region: z[0] == x[0], z[i] - z[i-1] == x[i] for every i >= 1 (int32
+    two's-complement arithmetic, as the scan's own wrap) and z[-1] == the
+    input total mod 2^32.  Together these pin z == cumsum(x) exactly."""
+    import torch
+
+    n = x.numel()
+    ok = int(z[0]) == int(x[0])
+    chunk = 1 << 26
+    for a in range(1, n, chunk):
+        b = min(n, a + chunk)
+        d = z[a:b] - z[a - 1:b - 1]  # int32, wraps like the scan itself
+        ok = ok and bool(torch.equal(d, x[a:b].to(torch.int32)))
+    tot = int(x.to(torch.int64).sum().item())
+    ok = ok and int(z[-1]) == ((tot + 2 ** 31) % 2 ** 32) - 2 ** 31
+    return ok
+
+
 def max_over_ranks(value, world, device):
     """Largest `value` over all ranks (the slowest rank's time); identity on one rank."""
     if world <= 1:
@@ -550,19 +627,29 @@ def cpu_reference_scan(n_sample, steps, warmup, seed=0):
                       f"mean {statistics.mean(times) * 1e3:.1f} ms/run, 512 MB cache flush between runs"}, times
 
 
+def headline_config(op, n, world):
+    """The workload description shared by both arms (identical dicts)."""
+    dname = OPS[op][0]
+    return {"workload": OPS[op][2], "n": n, "parallelism": f"replicas{world}",
+            "l2": "inputs larger than L2 (no flush needed)",
+            "input": "uniform int in [-8,8]" if dname == "int8" else "uniform[-1,1) fp16"}
+
+
 def run_reference_arm(args):
+    """The reference's own CPU scan (run_scan_cpu, src/torch/torch_scan_cpu.h)
+    on the full headline input (int8, n = 2^28), every step one call on all
+    host threads with a 512 MB cache flush before it."""
     world, rank, _ = dist_setup()
     if rank != 0:
         return 0
-    n = 1 << 28
-    sample = min(n, 1 << 26)
-    base, times = cpu_reference_scan(sample, max(args.steps, 1), max(args.warmup, 0))
+    n = args.n
+    base, times = cpu_reference_scan(n, max(args.steps, 1), max(args.warmup, 0))
     line = {
         "impl": "reference", "metric": METRIC, "value": base["value"], "unit": "elem/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": statistics.mean(times) * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "s8->s32", "data": "synthetic",
-        "config": {"workload": OPS["scan_i8"][2], "n": n, "sample_n": sample, "S": 64,
-                   "note": "reference run_scan_cpu (src/torch/torch_scan_cpu.h) on the host cores"},
+        "config": headline_config("scan_i8", n, world),
+        "note": "reference run_scan_cpu (src/torch/torch_scan_cpu.h) on the host cores, full input every step",
         "cpu_baseline": base,
         "e2e": {"value": base["value"], "unit": "elem/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -572,7 +659,7 @@ def run_reference_arm(args):
 
 PROFILE_OPS = ("compress_f16", "compress_f32", "compress_ind_f16", "spmv_f32", "spmv_f16", "serve", "segscan_i8",
                "segscan_f16", "segsum_i8", "segsum_f16", "segsum_f32", "split_f16", "sort_f16", "topk_f16",
-               "rowsum_f16")
+               "rowsum_f16", "scan_i8", "scan_f16", "scan_f32", "segflags_f16")
 
 
 def run_profile_op(args, dev):
@@ -587,7 +674,37 @@ def run_profile_op(args, dev):
     from tcuscan_b200 import serve, workloads
 
     op, n = args.profile_op, args.n
-    if op.startswith("compress"):
+    if op in ("scan_i8", "scan_f16", "scan_f32", "segflags_f16"):
+        # plain scans (S from --S, 0 = tuned) and the flag-driven segmented
+        # scan (start flags Bernoulli(0.01)); fp32 input is N(0, 1)
+        dt = {"i8": torch.int8, "f16": torch.float16, "f32": torch.float32}[op.split("_")[1]]
+        if dt == torch.float32:
+            xv = torch.randn(n, device=dev, generator=torch.Generator(device=dev).manual_seed(5))
+        else:
+            xv = workloads.scan_input(n, dt, dev, seed=5)
+        S = tcuscan_ops._pick_S(args.S or None, dt, n)
+        eb = xv.element_size()
+        if op == "segflags_f16":
+            fl = workloads.bernoulli_mask(n, 0.01, dev, seed=13)
+            fn = lambda: tcuscan_ops.run_seg_scan(xv, fl, 64)  # noqa: E731
+            nbytes = n * (eb + 1 + 4)
+        else:
+            fn = lambda: tcuscan_ops.run_scan_multi_core(xv, S)  # noqa: E731
+            nbytes = n * (eb + 4)
+        units = n
+        if args.phases:
+            from tcuscan_ops import _lib as L
+
+            fn()
+            torch.cuda.synchronize()
+            L.phase_times(dev, clear=True)
+            L.set_phase_profile(True)
+            for _ in range(5):
+                fn()
+            torch.cuda.synchronize()
+            L.set_phase_profile(False)
+            print(json.dumps({"phases_ns_sum_over_5_launches": L.phase_times(dev, clear=True)}), flush=True)
+    elif op.startswith("compress"):
         dt = torch.float32 if op == "compress_f32" else torch.float16
         mask = workloads.bernoulli_mask(n, 0.3, dev, seed=8)
         k = int(mask.sum().item())
@@ -731,7 +848,7 @@ def main():
 
     import tcuscan_ops
 
-    dname, bpe, desc = OPS[args.op]
+    dname, bpe, _ = OPS[args.op]
     n = args.n
     if not args.S:
         args.S = tcuscan_ops._pick_S(None, torch.int8 if dname == "int8" else torch.float16, n)
@@ -793,6 +910,22 @@ def main():
     sampler.stop()
 
     total_ms = max_over_ranks(total_ms, world, dev)
+
+    # ---- the timed output, checked once on the device outside the timed region ----
+    z = step()
+    torch.cuda.synchronize()
+    if dname == "int8":
+        check = {"exact": verify_headline(x, z), "method": "z[0] == x[0], diff(z) == x[1:] (int32), z[-1] == sum(x)"}
+        if not check["exact"]:
+            raise RuntimeError("headline scan output differs from cumsum(x)")
+    else:
+        ref = torch.cumsum(x.double(), 0)
+        err = ((z.double() - ref).abs() / ref.abs().clamp_min(1.0)).max().item()
+        check = {"max_rel_err_vs_fp64": err, "method": "FP64 cumsum on the device, floor max(|ref|, 1)"}
+        del ref
+        if err > 1e-3:
+            raise RuntimeError(f"headline scan error {err} above 1e-3")
+    del z
 
     # ---- e2e through the public API with host buffers: the host-buffer scan
     # (tcuscan_b200.stream) copies each 2^24-element chunk in, scans it and
@@ -865,8 +998,7 @@ def main():
 
     cpu_base = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        sample = min(n, 1 << 26)
-        cpu_base, _ = cpu_reference_scan(sample, 10, 2)
+        cpu_base, _ = cpu_reference_scan(n, 5, 1)
 
     if world > 1:
         torch.distributed.barrier()
@@ -892,9 +1024,9 @@ def main():
         "vs_baseline": None,
         "dtype": "s8->s32" if dname == "int8" else "f16->f32",
         "data": "synthetic",
-        "config": {"workload": desc, "n": n, "S": args.S, "parallelism": f"replicas{world}",
-                   "l2": "inputs larger than L2 (no flush needed)",
-                   "input": "uniform int in [-8,8]" if dname == "int8" else "uniform[-1,1) fp16"},
+        "config": headline_config(args.op, n, world),
+        "tile_S": args.S,
+        "check": check,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_kind": peak_kind, "frac_of_spec_8TBs": achieved / SPEC_HBM_GBS,
                      "traffic": profile_traffic(args.op), "algorithmic_bytes_per_launch": alg_bytes,
@@ -908,8 +1040,10 @@ def main():
         "clocks": clocks,
         "gpu_launches": args.steps,
         "median_ms_per_launch": statistics.median(per),
-        "extras": extras,
+        "legs": legs_summary(extras),
     }
+    if extras is not None:
+        print(json.dumps({"extras": extras}), flush=True)
     print(json.dumps(line), flush=True)
     return 0
 

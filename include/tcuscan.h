@@ -132,6 +132,16 @@ TCU_API tcu_status_t tcu_scan_chained(const void* x, tcu_dtype_t x_dtype, int64_
 TCU_API tcu_status_t tcu_scan_noalloc(const void* x, tcu_dtype_t x_dtype, int64_t n, int S, double start, void* z,
                                       void* stream);
 
+/* Host-side inclusive scan of a host array (x and z in host memory; no GPU
+ * work): int8 -> int32 (two's-complement wrap), fp16 / fp32 -> fp32.  The
+ * input is cut into min(threads, n) contiguous blocks, each scanned
+ * sequentially in the output type, the block totals scanned serially and
+ * each block's offset added (skipped where it is zero), so the results are
+ * bit-identical to the reference's for the same block count (it uses
+ * omp_get_max_threads()).  n <= 2^32 - 1.  Synchronous.
+ * Replaces run_scan_cpu (src/torch/torch_scan_cpu.h:24-107).              */
+TCU_API tcu_status_t tcu_scan_cpu(const void* x, tcu_dtype_t x_dtype, int64_t n, void* z, int threads);
+
 /* Per-row scans of n_rows rows of S elements (z has n_rows*S elements).
  * Replaces run_row_scan (src/torch/torch_scan.h:312-351).                 */
 TCU_API tcu_status_t tcu_row_scan(const void* x, tcu_dtype_t x_dtype, int64_t n_rows, int S, void* z, void* ws,

@@ -836,14 +836,30 @@ def run_spmv_multi_cube(vals, indptr, cols, x, upper, lower_strict):
 
 
 def run_scan_cpu(x):
-    """The reference's CPU scan API (src/torch/torch_scan_cpu.h:88-107):
-    float16/float32 -> float32, int8 -> int32, computed on the host.  This is
-    a CPU operator of the reference's interface, not a fallback for any CUDA
-    operator above."""
+    """The reference's CPU scan (src/torch/torch_scan_cpu.h:24-107) on a host
+    tensor: float16/float32 -> float32, int8 -> int32.
+
+    Runs the library's host scan (tcu_scan_cpu) with the reference's blocked
+    three-phase order: torch.get_num_threads() contiguous blocks (the
+    reference uses omp_get_max_threads(), the same count in a torch process),
+    each scanned sequentially in the output type, then the serial scan of the
+    block totals added per block, so fp32 results round exactly as the
+    reference's do for the same thread count.  This is a CPU operator of the
+    reference's interface, not a fallback for any CUDA operator above."""
+    if not isinstance(x, torch.Tensor):
+        raise TypeError("x must be a torch.Tensor")
     if x.device.type != "cpu":
         raise ValueError("run_scan_cpu expects a CPU tensor")
-    out = torch.float32 if x.dtype in (torch.float16, torch.float32) else torch.int32
-    return torch.cumsum(x.to(out), dim=0)
+    if x.dtype not in (torch.int8, torch.float16, torch.float32):
+        raise TypeError(f"unsupported dtype {x.dtype}: run_scan_cpu takes int8, float16 or float32")
+    x = x.contiguous().reshape(-1)
+    out = torch.empty(x.numel(), dtype=torch.int32 if x.dtype == torch.int8 else torch.float32)
+    if x.numel() == 0:
+        return out
+    st = _lib.lib.tcu_scan_cpu(x.data_ptr(), _lib.DTYPE_CODE[x.dtype], x.numel(), out.data_ptr(),
+                               torch.get_num_threads())
+    check(st, "run_scan_cpu")
+    return out
 
 
 __all__ = [n for n in dir() if n.startswith("run_")] + ["TcuError", "workspace_error", "raise_device_error"]

@@ -68,6 +68,7 @@ _sig("tcu_selftest_wait_timeout", _ST, _I, _U64, _P, _SZ, _P)
 _sig("tcu_get_max_ctas", _I)
 _sig("tcu_workspace_phase_ns", _ST, _P, ctypes.POINTER(ctypes.c_uint64), _I, _P)
 _sig("tcu_scan", _ST, _P, _I, _I64, _I, _D, _P, _P, _SZ, _P)
+_sig("tcu_scan_cpu", _ST, _P, _I, _I64, _P, _I)
 _sig("tcu_scan_chained", _ST, _P, _I, _I64, _I, _D, _P, _P, _P, _SZ, _P)
 _sig("tcu_row_scan", _ST, _P, _I, _I64, _I, _P, _P, _SZ, _P)
 _sig("tcu_block_scan", _ST, _P, _I, _I64, _I, _P, _P, _SZ, _P)

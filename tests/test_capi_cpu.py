@@ -5,6 +5,7 @@ import glob
 import os
 import re
 
+import numpy as np
 import pytest
 import torch
 
@@ -152,6 +153,56 @@ def test_run_scan_cpu_api():
     assert torch.equal(tcuscan_ops.run_scan_cpu(x), torch.cumsum(x, 0, dtype=torch.int32))
     xf = torch.randn(1000).half()
     assert tcuscan_ops.run_scan_cpu(xf).dtype == torch.float32
+    assert tcuscan_ops.run_scan_cpu(torch.empty(0, dtype=torch.float32)).numel() == 0
+    with pytest.raises(TypeError):
+        tcuscan_ops.run_scan_cpu(torch.zeros(4, dtype=torch.float64))
+
+
+def test_run_scan_cpu_matches_reference_fixtures(golden):
+    """run_scan_cpu against the reference's own run_scan_cpu outputs (golden
+    fixtures, made with the thread count they record): bit-exact for int8,
+    fp16 and fp32 when the block count is the same."""
+    import tcuscan_ops
+
+    threads = int(golden["scan_threads"])
+    keys = sorted({k[:-4] for k in golden.files if k.startswith("scan_") and k.endswith("_ref")
+                   and k.split("_")[1] in ("i8", "f16", "f32")})
+    assert keys
+    old = torch.get_num_threads()
+    try:
+        torch.set_num_threads(threads)
+        for b in keys:
+            x, ref = golden[b + "_x"], golden[b + "_ref"]
+            got = tcuscan_ops.run_scan_cpu(torch.from_numpy(x)).numpy()
+            assert got.dtype == ref.dtype, b
+            assert np.array_equal(got.view(np.uint32), ref.view(np.uint32)), b
+    finally:
+        torch.set_num_threads(old)
+
+
+@pytest.mark.parametrize("threads", [1, 3, 16])
+@pytest.mark.parametrize("dtype", [torch.int8, torch.float16, torch.float32])
+def test_run_scan_cpu_blocked_order(threads, dtype):
+    """Same rounding as the oracle's restatement of the reference's blocked
+    scan for any block count, across the worker threshold (2^16 elements)."""
+    import oracle
+    import tcuscan_ops
+
+    g = torch.Generator().manual_seed(threads)
+    for n in (1, 5, 1000, (1 << 16) + 3):
+        if dtype == torch.int8:
+            x = torch.randint(-128, 128, (n,), dtype=torch.int8, generator=g)
+            want = oracle.blocked_scan_like_reference(x.numpy().astype(np.int32), threads)
+        else:
+            x = (torch.randn(n, generator=g) * 100).to(dtype)
+            want = oracle.blocked_scan_like_reference(x.numpy().astype(np.float32), threads)
+        old = torch.get_num_threads()
+        try:
+            torch.set_num_threads(threads)
+            got = tcuscan_ops.run_scan_cpu(x).numpy()
+        finally:
+            torch.set_num_threads(old)
+        assert np.array_equal(got.view(np.uint32), np.asarray(want).view(np.uint32)), (n, threads)
 
 
 def test_tcuscan_package_reexports():

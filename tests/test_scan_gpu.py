@@ -162,14 +162,16 @@ def test_block_scan(S, m):
     assert oracle.max_rel_err(z, ref) < 1e-5
 
 
-def test_scan_full_size_int8_property():
-    """n = 2^28 int8: z[0] == x[0] and diff(z) == x[1:] exactly, which pins z = cumsum(x)."""
+@pytest.mark.parametrize("S", [64, 128, None])
+def test_scan_full_size_int8_property(S):
+    """n = 2^28 int8: z[0] == x[0] and diff(z) == x[1:] exactly, which pins z = cumsum(x).
+    S = 128 and S = None (autotuned) are the benchmark's headline configuration."""
     import tcuscan_ops
 
     n = 1 << 28
     g = torch.Generator(device=DEV).manual_seed(0)
     x = torch.randint(-8, 9, (n,), dtype=torch.int8, device=DEV, generator=g)
-    z = tcuscan_ops.run_scan_multi_core(x, 64)
+    z = tcuscan_ops.run_scan_multi_core(x, S)
     tcuscan_ops.raise_device_error(x.device)
     assert int(z[0]) == int(x[0])
     d = torch.diff(z)
@@ -177,14 +179,15 @@ def test_scan_full_size_int8_property():
     assert int(z[-1]) == int(x.to(torch.int64).sum())
 
 
-def test_scan_full_size_fp16_vs_fp64():
+@pytest.mark.parametrize("S", [64, None])
+def test_scan_full_size_fp16_vs_fp64(S):
     """n = 2^28 fp16 uniform[-1,1): max rel error vs an FP64 cumsum <= 1e-3."""
     import tcuscan_ops
 
     n = 1 << 28
     g = torch.Generator(device=DEV).manual_seed(0)
     x = (torch.rand(n, device=DEV, generator=g) * 2 - 1).half()
-    z = tcuscan_ops.run_scan_multi_core(x, 64)
+    z = tcuscan_ops.run_scan_multi_core(x, S)
     tcuscan_ops.raise_device_error(x.device)
     ref = torch.cumsum(x.double(), 0)
     err = ((z.double() - ref).abs() / ref.abs().clamp_min(1.0)).max().item()
