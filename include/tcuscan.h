@@ -90,6 +90,12 @@ TCU_API tcu_status_t tcu_selftest_wait_timeout(int which, uint64_t timeout_ns, v
  * Process-wide; the autotuner sets it per size class. */
 TCU_API void tcu_set_max_ctas(int n);
 TCU_API int tcu_get_max_ctas(void);
+/* Tuning: full scans of n elements run with one 128 x S block per look-back
+ * tile (instead of 32768-element tiles) when ceil(n / 32768) < `tiles`, so
+ * small inputs spread over every SM.  Default (or a negative value): the SM
+ * count; 0 disables the small tiles.  Process-wide. */
+TCU_API void tcu_set_small_tile_limit(int tiles);
+TCU_API int tcu_get_small_tile_limit(void);
 TCU_API tcu_status_t tcu_workspace_phase_ns(void* ws, uint64_t out[8], int clear, void* stream);
 
 /* ---- scans ---------------------------------------------------------------
@@ -113,6 +119,24 @@ TCU_API tcu_status_t tcu_scan(const void* x, tcu_dtype_t x_dtype, int64_t n, int
  * (used to overlap host copies with the scan, tcuscan_b200.stream).        */
 TCU_API tcu_status_t tcu_scan_chained(const void* x, tcu_dtype_t x_dtype, int64_t n, int S, double start,
                                       const void* start_dev, void* z, void* ws, size_t ws_bytes, void* stream);
+
+/* tcu_scan_chained with the device start value's type given: start_dtype
+ * TCU_INT32, TCU_INT64, TCU_FLOAT32 or TCU_FLOAT64 (start_dev aligned to its
+ * size).  No reference counterpart: the sharded scan passes the exclusive
+ * prefix of the ranks' totals as int64 (int8 input) or FP64 (fp16 / fp32
+ * input), so the carry between ranks keeps the precision of the carry chain
+ * inside one GPU.                                                          */
+TCU_API tcu_status_t tcu_scan_chained_typed(const void* x, tcu_dtype_t x_dtype, int64_t n, int S, double start,
+                                            const void* start_dev, tcu_dtype_t start_dtype, void* z, void* ws,
+                                            size_t ws_bytes, void* stream);
+
+/* Sum of all n elements of x into *out (8-byte aligned device memory):
+ * int8 -> int64 (exact), fp16 / fp32 -> FP64, in a fixed order (the same
+ * bits on every call).  ws: a workspace of at least tcu_workspace_bytes(n, S)
+ * bytes for any S (its scratch is zeroed again by the call).  No reference
+ * counterpart: the exchange step of the sharded scan (one total per rank). */
+TCU_API tcu_status_t tcu_total(const void* x, tcu_dtype_t dtype, int64_t n, void* out, void* ws, size_t ws_bytes,
+                               void* stream);
 
 /* Inclusive scan that allocates nothing.  No counterpart in the reference.
  * Same arguments and results as tcu_scan, minus the workspace, for callers

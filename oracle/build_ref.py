@@ -6,6 +6,9 @@ checkout (never copied).  Output goes to oracle/_ref/ only.  Usage:
 
     python oracle/build_ref.py [--ref /path/to/reference]
 
+The checkout is found from --ref, else the TCUSCAN_REFERENCE environment
+variable, else a directory named ``reference`` next to this repository.
+
 The built module is test infrastructure: tests/golden/make_golden.py uses it to
 pin the oracle, and bench.py's CPU baseline times it.  Machines without the
 reference checkout only load the prebuilt .so.
@@ -17,7 +20,16 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
-DEFAULT_REF = "/root/reference"
+
+
+def reference_root(ref=None):
+    """The reference checkout: `ref`, else $TCUSCAN_REFERENCE, else the
+    ``reference`` directory beside this repository; None if none exists."""
+    for cand in (ref, os.environ.get("TCUSCAN_REFERENCE"),
+                 os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference")):
+        if cand and os.path.isdir(os.path.join(cand, "src")):
+            return cand
+    return None
 
 
 def built_module_path():
@@ -25,7 +37,10 @@ def built_module_path():
     return hits[0] if hits else None
 
 
-def build(ref_root=DEFAULT_REF, verbose=False):
+def build(ref_root=None, verbose=False):
+    ref_root = reference_root(ref_root)
+    if ref_root is None:
+        raise FileNotFoundError("reference checkout not found (pass --ref or set TCUSCAN_REFERENCE)")
     header_dir = os.path.join(ref_root, "src", "torch")
     if not os.path.exists(os.path.join(header_dir, "torch_scan_cpu.h")):
         raise FileNotFoundError(f"reference CPU scan header not found under {header_dir}")
@@ -65,7 +80,7 @@ def load_module():
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default=DEFAULT_REF)
+    ap.add_argument("--ref", default=None)
     ap.add_argument("-v", action="store_true")
     a = ap.parse_args()
     p = build(a.ref, a.v)

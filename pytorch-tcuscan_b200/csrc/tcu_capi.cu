@@ -147,8 +147,9 @@ constexpr tcu_dtype_t kDtypeSplitF32 = (tcu_dtype_t)100;
 template <typename InT, int W, int MODE>
 static tcu_status_t launch_scan_tc(const void* x, int64_t n, void* z, double start_f, long long start_i,
                                    int seg_rows, void* ws, size_t ws_bytes, cudaStream_t st,
-                                   const SegArgs& sa = SegArgs(), const void* start_dev = nullptr) {
-  using C = ScanCfg<InT, W, is_seg(MODE)>;
+                                   const SegArgs& sa = SegArgs(), const void* start_dev = nullptr,
+                                   int start_dev_kind = 0) {
+  using C = ScanCfg<InT, W, is_seg(MODE), MODE == kScanFullSmall>;
   ScanParams p{};
   p.x = x;
   p.z = z;
@@ -162,6 +163,7 @@ static tcu_status_t launch_scan_tc(const void* x, int64_t n, void* z, double sta
   p.start_f = start_f;
   p.start_i = start_i;
   p.start_dev = start_dev;
+  p.start_dev_kind = start_dev_kind;
   p.timeout_ns = g_timeout_ns;
   if (ws == nullptr || ws_capacity(ws_bytes) < p.num_tiles) {
     snprintf(g_errmsg, sizeof(g_errmsg), "workspace too small: %lld tiles need %zu bytes", (long long)p.num_tiles,
@@ -229,28 +231,44 @@ static tcu_status_t launch_scan_tc(const void* x, int64_t n, void* z, double sta
   return TCU_OK;
 }
 
+// Full scans whose 32768-element tiles would leave SMs idle run with one
+// 128 x S block per tile instead (kScanFullSmall).  The limit is in default
+// tiles; tcu_set_small_tile_limit changes it (0 = never).
+static int g_small_tile_limit = -1;  // -1: the SM count
+static bool use_small_tiles(int64_t n) {
+  const int64_t lim = g_small_tile_limit < 0 ? (int64_t)sm_count() : (int64_t)g_small_tile_limit;
+  return (n + 32767) / 32768 < lim;
+}
+
 template <int MODE>
 static tcu_status_t dispatch_scan(const void* x, tcu_dtype_t dt, int64_t n, int S, void* z, double start, int seg_rows,
-                                  void* ws, size_t ws_bytes, cudaStream_t st, const void* start_dev = nullptr) {
+                                  void* ws, size_t ws_bytes, cudaStream_t st, const void* start_dev = nullptr,
+                                  int sk = -1) {
+  if (sk < 0) sk = dt == TCU_INT8 ? 0 : 1;  // default device start: an output element (int32 / fp32)
+  if constexpr (MODE == kScanFull) {
+    if (use_small_tiles(n))
+      return dispatch_scan<kScanFullSmall>(x, dt, n, S, z, start, seg_rows, ws, ws_bytes, st, start_dev, sk);
+  }
   const long long si = (long long)start;
   if (dt == TCU_INT8) {
     switch (S) {
-      case 32: return launch_scan_tc<int8_t, 32, MODE>(x, n, z, 0.0, si, seg_rows, ws, ws_bytes, st, SegArgs(), start_dev);
-      case 64: return launch_scan_tc<int8_t, 64, MODE>(x, n, z, 0.0, si, seg_rows, ws, ws_bytes, st, SegArgs(), start_dev);
-      case 128: return launch_scan_tc<int8_t, 128, MODE>(x, n, z, 0.0, si, seg_rows, ws, ws_bytes, st, SegArgs(), start_dev);
+      case 32: return launch_scan_tc<int8_t, 32, MODE>(x, n, z, 0.0, si, seg_rows, ws, ws_bytes, st, SegArgs(), start_dev, sk);
+      case 64: return launch_scan_tc<int8_t, 64, MODE>(x, n, z, 0.0, si, seg_rows, ws, ws_bytes, st, SegArgs(), start_dev, sk);
+      case 128: return launch_scan_tc<int8_t, 128, MODE>(x, n, z, 0.0, si, seg_rows, ws, ws_bytes, st, SegArgs(), start_dev, sk);
       default: return TCU_ERR_ARG;
     }
   }
-  if (dt == TCU_FLOAT32) {  // split-precision bf16 hi + lo operands, 64-column rows
-    if (MODE != kScanFull) return TCU_ERR_DTYPE;
-    return launch_scan_tc<float, 64, kScanFull>(x, n, z, start, 0, seg_rows, ws, ws_bytes, st, SegArgs(), start_dev);
+  if (dt == TCU_FLOAT32) {  // split-precision fp16 hi + lo operands, 64-column rows
+    if constexpr (is_full(MODE))
+      return launch_scan_tc<float, 64, MODE>(x, n, z, start, 0, seg_rows, ws, ws_bytes, st, SegArgs(), start_dev, sk);
+    return TCU_ERR_DTYPE;
   }
   if (dt == TCU_FLOAT16) {
     switch (S) {
-      case 16: return launch_scan_tc<__half, 16, MODE>(x, n, z, start, 0, seg_rows, ws, ws_bytes, st, SegArgs(), start_dev);
-      case 32: return launch_scan_tc<__half, 32, MODE>(x, n, z, start, 0, seg_rows, ws, ws_bytes, st, SegArgs(), start_dev);
-      case 64: return launch_scan_tc<__half, 64, MODE>(x, n, z, start, 0, seg_rows, ws, ws_bytes, st, SegArgs(), start_dev);
-      case 128: return launch_scan_tc<__half, 128, MODE>(x, n, z, start, 0, seg_rows, ws, ws_bytes, st, SegArgs(), start_dev);
+      case 16: return launch_scan_tc<__half, 16, MODE>(x, n, z, start, 0, seg_rows, ws, ws_bytes, st, SegArgs(), start_dev, sk);
+      case 32: return launch_scan_tc<__half, 32, MODE>(x, n, z, start, 0, seg_rows, ws, ws_bytes, st, SegArgs(), start_dev, sk);
+      case 64: return launch_scan_tc<__half, 64, MODE>(x, n, z, start, 0, seg_rows, ws, ws_bytes, st, SegArgs(), start_dev, sk);
+      case 128: return launch_scan_tc<__half, 128, MODE>(x, n, z, start, 0, seg_rows, ws, ws_bytes, st, SegArgs(), start_dev, sk);
       default: return TCU_ERR_ARG;
     }
   }
@@ -303,6 +321,8 @@ const char* tcu_last_error_message(void) { return g_errmsg; }
 
 void tcu_set_phase_profile(int enable) { g_phase_profile = enable ? 1 : 0; }
 void tcu_set_max_ctas(int n) { g_max_ctas = n > 0 ? n : 0; }
+void tcu_set_small_tile_limit(int tiles) { g_small_tile_limit = tiles < 0 ? -1 : tiles; }
+int tcu_get_small_tile_limit(void) { return g_small_tile_limit < 0 ? sm_count() : g_small_tile_limit; }
 int tcu_get_max_ctas(void) { return g_max_ctas; }
 
 tcu_status_t tcu_workspace_phase_ns(void* ws, uint64_t out[8], int clear, void* stream) {
@@ -363,11 +383,28 @@ tcu_status_t tcu_selftest_wait_timeout(int which, uint64_t timeout_ns, void* ws,
 
 tcu_status_t tcu_scan_chained(const void* x, tcu_dtype_t x_dtype, int64_t n, int S, double start,
                               const void* start_dev, void* z, void* ws, size_t ws_bytes, void* stream) {
+  return tcu_scan_chained_typed(x, x_dtype, n, S, start, start_dev, x_dtype == TCU_INT8 ? TCU_INT32 : TCU_FLOAT32, z,
+                                ws, ws_bytes, stream);
+}
+
+tcu_status_t tcu_scan_chained_typed(const void* x, tcu_dtype_t x_dtype, int64_t n, int S, double start,
+                                    const void* start_dev, tcu_dtype_t start_dtype, void* z, void* ws,
+                                    size_t ws_bytes, void* stream) {
   if (n < 0) return TCU_ERR_ARG;
   if (n == 0) return TCU_OK;
   if (!x || !z) return TCU_ERR_ARG;
-  if (!aligned16(x) || !aligned16(z) || (reinterpret_cast<uintptr_t>(start_dev) & 3u)) return TCU_ERR_ALIGN;
-  return dispatch_scan<kScanFull>(x, x_dtype, n, S, z, start, 0, ws, ws_bytes, (cudaStream_t)stream, start_dev);
+  int sk;
+  switch (start_dtype) {
+    case TCU_INT32: sk = 0; break;
+    case TCU_FLOAT32: sk = 1; break;
+    case TCU_INT64: sk = 2; break;
+    case TCU_FLOAT64: sk = 3; break;
+    default: return TCU_ERR_DTYPE;
+  }
+  const uintptr_t amask = sk >= 2 ? 7u : 3u;
+  if (!aligned16(x) || !aligned16(z) || (reinterpret_cast<uintptr_t>(start_dev) & amask)) return TCU_ERR_ALIGN;
+  if (x_dtype == TCU_INT8 && S == 16) S = 32;
+  return dispatch_scan<kScanFull>(x, x_dtype, n, S, z, start, 0, ws, ws_bytes, (cudaStream_t)stream, start_dev, sk);
 }
 
 tcu_status_t tcu_scan(const void* x, tcu_dtype_t x_dtype, int64_t n, int S, double start, void* z, void* ws,

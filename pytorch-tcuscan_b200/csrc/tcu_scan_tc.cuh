@@ -48,8 +48,10 @@ enum ScanMode : int {
   kSegEnds = 4,      // segmented scan, int8 flags mark segment ends (seg_sum)
   kSegBounds = 5,    // segments from a sorted start array (indptr / offsets)
   kSegPeriodic = 6,  // segments of a fixed length (scan_batch)
+  kScanFullSmall = 7,  // kScanFull with one 128 x W block per tile (small inputs: every SM gets a tile)
 };
-constexpr bool is_seg(int mode) { return mode >= kSegFlags; }
+constexpr bool is_seg(int mode) { return mode >= kSegFlags && mode <= kSegPeriodic; }
+constexpr bool is_full(int mode) { return mode == kScanFull || mode == kScanFullSmall; }
 
 struct ScanParams {
   const void* x;      // input base (tail row loads)
@@ -61,7 +63,8 @@ struct ScanParams {
   int64_t num_tiles;
   double start_f;     // starting value (run_scan_single_core's starting_sum)
   long long start_i;
-  const void* start_dev;  // optional: one output element (int32 / fp32) added to the start (chained chunks)
+  const void* start_dev;  // optional: one value added to the start, read when the kernel runs (chained chunks)
+  int start_dev_kind;     // its type: 0 int32, 1 fp32, 2 int64, 3 fp64
   WsHeader* ws;
   TileDesc* descs;
   uint64_t timeout_ns;
@@ -90,11 +93,14 @@ constexpr uint32_t kSentinel = 0xFFFFFFFFu;
 constexpr int kThreads = 384;  // 12 warps: producer, MMA, 2 epilogue warpgroups, summer, second fp32 converter
 constexpr int kMaxSmem = 232448;
 
-template <typename InT, int W, bool SEG = false>
+template <typename InT, int W, bool SEG = false, bool SMALL = false>
 struct ScanCfg {
   static constexpr int IN_BYTES = (int)sizeof(InT);   // input element bytes
-  static constexpr bool IS_F32 = (IN_BYTES == 4);     // fp32: split into bf16 hi + lo operands
-  static constexpr bool PRESPLIT = __is_same(InT, SplitF32);  // ... already split in memory
+  static constexpr bool IS_F32 = (IN_BYTES == 4);     // fp32: split into two 16-bit operands
+  static constexpr bool PRESPLIT = __is_same(InT, SplitF32);  // ... already split in memory (bf16 hi + lo)
+  // fp32 input split in SMEM into scaled fp16 hi + lo operands, with every
+  // row's exact total computed from the fp32 values (convert_f32_rows)
+  static constexpr bool F16SPLIT = IS_F32 && !PRESPLIT;
   static constexpr int ELEM = IS_F32 ? 2 : IN_BYTES;  // MMA operand element bytes
   static constexpr bool IS_INT = (IN_BYTES == 1);
   static constexpr int RB = W * ELEM;                 // operand row bytes
@@ -106,12 +112,14 @@ struct ScanCfg {
   static constexpr int IN_KB = IN_RB / IN_SW;
   static constexpr int STAGE_BYTES = 128 * IN_RB;
   static constexpr int TERM_BYTES = 128 * RB;         // fp32: hi operand at 0, lo at TERM_BYTES
-  static constexpr int BPT = 256 / W;                 // blocks per tile
-  static constexpr int TILE_ELEMS = 128 * 256;
+  static constexpr int BPT = SMALL ? 1 : 256 / W;     // blocks per tile
+  static constexpr int TILE_ELEMS = 128 * W * BPT;
   static constexpr int B_BYTES = W * RB;
   static constexpr int OBW = W < 32 ? W : 32;         // output TMA box width (elements)
   static constexpr int OSW = OBW * 4;                 // output box row bytes = swizzle span
-  static constexpr int FILLW = W < 64 ? W : 64;       // columns staged per fill
+  // columns staged per fill: 64, or 32 for the fp32 full scan (a smaller
+  // staging area leaves room for a fifth input stage)
+  static constexpr int FILLW = (F16SPLIT && !SEG) ? 32 : (W < 64 ? W : 64);
   static constexpr int NFILL = W / FILLW;
   static constexpr int STG_BYTES = 128 * FILLW * 4;
   // Shared memory: input stage ring | U | output staging | control.  The ring
@@ -122,7 +130,11 @@ struct ScanCfg {
   static constexpr int B_ALLOC = ((B_BYTES + 1023) / 1024) * 1024;
   // segmented modes keep one 64-bit start mask per row of a tile per warpgroup
   static constexpr int MASK_BYTES = SEG ? 2 * BPT * 128 * 8 : 0;
-  static constexpr int FIXED = 1024 + CTRL_BYTES + B_ALLOC + MASK_BYTES;
+  // F16SPLIT: per row of a tile per warpgroup, the power-of-two factor that
+  // undoes the row's operand scale (float) and the row's exact total (double)
+  static constexpr int RS_BYTES = F16SPLIT ? 2 * BPT * 128 * 4 : 0;
+  static constexpr int RT_BYTES = F16SPLIT ? 2 * BPT * 128 * 8 : 0;
+  static constexpr int FIXED = 1024 + CTRL_BYTES + B_ALLOC + MASK_BYTES + RS_BYTES + RT_BYTES;
   static constexpr int NST_DOUBLE = (kMaxSmem - FIXED - 4 * STG_BYTES) / STAGE_BYTES;
   static constexpr int STG_BUFS = NST_DOUBLE >= 2 * BPT ? 2 : 1;
   static constexpr int NST_FIT = (kMaxSmem - FIXED - 2 * STG_BUFS * STG_BYTES) / STAGE_BYTES;
@@ -131,7 +143,9 @@ struct ScanCfg {
   static constexpr int OFF_B = NSTAGE * STAGE_BYTES;
   static constexpr int OFF_STG = OFF_B + B_ALLOC;
   static constexpr int OFF_MASK = OFF_STG + 2 * STG_BUFS * STG_BYTES;
-  static constexpr int OFF_CTRL = OFF_MASK + MASK_BYTES;
+  static constexpr int OFF_RT = OFF_MASK + MASK_BYTES;  // double[2][BPT][128] (8-byte aligned)
+  static constexpr int OFF_RS = OFF_RT + RT_BYTES;      // float[2][BPT][128]
+  static constexpr int OFF_CTRL = OFF_RS + RS_BYTES;
   static constexpr int SMEM_BYTES = OFF_CTRL + CTRL_BYTES + 1024;  // + alignment slack
   static_assert(NSTAGE >= BPT, "stage ring must hold a whole tile");
   static_assert(!SEG || W == 32 || W == 64, "segmented modes use S = 32 or 64");
@@ -200,7 +214,14 @@ __device__ __forceinline__ float load_at(const void* x, int64_t e) {
 template <typename V, bool IS_INT, typename P>
 __device__ __forceinline__ V scan_start(const P& p) {
   V s = IS_INT ? (V)p.start_i : (V)p.start_f;
-  if (p.start_dev) s += IS_INT ? (V)*static_cast<const int*>(p.start_dev) : (V)*static_cast<const float*>(p.start_dev);
+  if (p.start_dev) {
+    switch (p.start_dev_kind) {
+      case 0: s += (V)*static_cast<const int*>(p.start_dev); break;
+      case 1: s += (V)*static_cast<const float*>(p.start_dev); break;
+      case 2: s += (V)*static_cast<const long long*>(p.start_dev); break;
+      default: s += (V)*static_cast<const double*>(p.start_dev); break;
+    }
+  }
   return s;
 }
 
@@ -212,54 +233,82 @@ __device__ __forceinline__ void seg_combine(int& f, V& v, int f_prev, V v_prev) 
   f |= f_prev;
 }
 
-// Split four fp32 values into bf16 hi = RN(x) and lo = RN(x - hi) (x - hi
-// is exact in fp32), packed four per uint2 in column order.
-__device__ __forceinline__ void split_bf16x4(const float4 v, uint2& hi, uint2& lo) {
-  const __nv_bfloat162 h01 = __floats2bfloat162_rn(v.x, v.y);
-  const __nv_bfloat162 h23 = __floats2bfloat162_rn(v.z, v.w);
-  const float2 f01 = __bfloat1622float2(h01), f23 = __bfloat1622float2(h23);
-  const __nv_bfloat162 l01 = __floats2bfloat162_rn(v.x - f01.x, v.y - f01.y);
-  const __nv_bfloat162 l23 = __floats2bfloat162_rn(v.z - f23.x, v.w - f23.y);
-  hi = make_uint2(*reinterpret_cast<const uint32_t*>(&h01), *reinterpret_cast<const uint32_t*>(&h23));
-  lo = make_uint2(*reinterpret_cast<const uint32_t*>(&l01), *reinterpret_cast<const uint32_t*>(&l23));
-}
-
-// In-place split of rows [4 * it_lo, 4 * it_hi) of an fp32 block: each
-// 64-column row arrives as two 128-byte halves (TMA boxes at +0 and
-// +term_bytes, same swizzle); the row is rewritten as 64 bf16 hi = RN(x) in
-// the first slot and 64 bf16 lo = RN(x - hi) in the second, the two MMA
-// operand tiles.  A row is fully read (8 lanes x 2 x 16 B) before any lane
-// writes it.  Rows in [r_lo, vrows) are also summed into acc: FP32 per lane
-// in two chains (at most 64 values each), the caller adds each stage's
-// partial to an FP64 aggregate.
-__device__ __forceinline__ void convert_f32_rows(uint8_t* X0, int term_bytes, int it_lo, int it_hi, int r_lo,
-                                                 int vrows, bool sums, float& acc) {
+// In-place split of rows [row0, row1) of an fp32 block into the two fp16
+// MMA operand tiles, with every row's exact total; one lane per row (32 rows
+// per pass, no cross-lane work).  Each 64-column row arrives as two 128-byte
+// halves (TMA boxes at +0 and +term_bytes, same swizzle) and is rewritten as
+// 64 fp16 hi in the first slot and 64 fp16 lo in the second.  For a row whose
+// largest |x| lies in [2^e, 2^(e+1)):
+//   y  = x * 2^k, k = 14 - e            (exact; |y| < 2^15)
+//   hi = y rounded to a multiple of 16  (|hi| / 16 <= 2048: exact in fp16)
+//   r  = y - hi                         (exact in fp32; |r| <= 8)
+//   lo = RN_fp16(r)                     (|r - lo| <= 2^-8 = 2^-22 of 2^14)
+// so hi + lo carries 22 significant bits of the row's scale, and the
+// epilogue multiplies the MMA result by 2^-k (exact).  The row total is
+// 2^-k * (sum hi + sum r): the hi sum is exact in fp32 (multiples of 16
+// below 2^21) and the r sum is within 2^-16 of 512 in fp32, combined in FP64
+// -- the total of the fp32 inputs themselves, not of their split, so the
+// carries between rows and tiles carry no split error.  rs_out[row] = 2^-k,
+// rt_out[row] = the total.  Rows in [r_lo, vrows) are also added to acc.
+// The lane loads its whole row before writing it.  Non-finite rows keep k = 0.
+__device__ __forceinline__ void convert_f32_rows(uint8_t* X0, int term_bytes, int row0, int row1, int r_lo,
+                                                 int vrows, bool sums, double& acc, float* rs_out,
+                                                 double* rt_out) {
   uint8_t* X1 = X0 + term_bytes;
   const int lane = threadIdx.x & 31;
-  const int rr = lane >> 3, cidx = lane & 7;
-  float c0 = 0.f, c1 = 0.f;
-#pragma unroll 4
-  for (int it = it_lo; it < it_hi; ++it) {
-    const int row = it * 4 + rr;
-    const uint32_t off = swz(row * 128 + cidx * 16, 128);
-    const float4 a = *reinterpret_cast<const float4*>(X0 + off);
-    const float4 b = *reinterpret_cast<const float4*>(X1 + off);
-    __syncwarp();
-    if (sums && row < vrows && row >= r_lo) {
-      const float v = ((a.x + a.y) + (a.z + a.w)) + ((b.x + b.y) + (b.z + b.w));
-      if (it & 1) c1 += v;
-      else c0 += v;
+  const float kRound16 = 201326592.0f;  // 1.5 * 2^27: (y + c) - c rounds y to a multiple of 16
+#pragma unroll 1
+  for (int row = row0 + lane; row < row1; row += 32) {
+    float v[64];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      const uint32_t off = swz(row * 128 + c * 16, 128);
+      const float4 a = *reinterpret_cast<const float4*>(X0 + off);
+      const float4 b = *reinterpret_cast<const float4*>(X1 + off);
+      v[4 * c] = a.x; v[4 * c + 1] = a.y; v[4 * c + 2] = a.z; v[4 * c + 3] = a.w;
+      v[32 + 4 * c] = b.x; v[33 + 4 * c] = b.y; v[34 + 4 * c] = b.z; v[35 + 4 * c] = b.w;
     }
-    uint2 ha, la, hb, lb;
-    split_bf16x4(a, ha, la);
-    split_bf16x4(b, hb, lb);
-    const int half = (cidx & 1) * 8;
-    *reinterpret_cast<uint2*>(X0 + swz(row * 128 + (cidx >> 1) * 16, 128) + half) = ha;
-    *reinterpret_cast<uint2*>(X0 + swz(row * 128 + (4 + (cidx >> 1)) * 16, 128) + half) = hb;
-    *reinterpret_cast<uint2*>(X1 + swz(row * 128 + (cidx >> 1) * 16, 128) + half) = la;
-    *reinterpret_cast<uint2*>(X1 + swz(row * 128 + (4 + (cidx >> 1)) * 16, 128) + half) = lb;
+    float mx[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      mx[q] = fmaxf(fmaxf(fabsf(v[8 * q]), fabsf(v[8 * q + 1])), fmaxf(fabsf(v[8 * q + 2]), fabsf(v[8 * q + 3])));
+      mx[q] = fmaxf(mx[q], fmaxf(fmaxf(fabsf(v[8 * q + 4]), fabsf(v[8 * q + 5])),
+                                 fmaxf(fabsf(v[8 * q + 6]), fabsf(v[8 * q + 7]))));
+    }
+    const float m = fmaxf(fmaxf(fmaxf(mx[0], mx[1]), fmaxf(mx[2], mx[3])),
+                          fmaxf(fmaxf(mx[4], mx[5]), fmaxf(mx[6], mx[7])));
+    const int eb = (int)((__float_as_uint(m) >> 23) & 0xFFu);  // biased exponent of the row's max
+    int k = eb == 0xFF ? 0 : 141 - eb;                          // 14 - (eb - 127)
+    k = k > 126 ? 126 : k;                                      // k >= -113 always
+    const float sc = __uint_as_float((uint32_t)(k + 127) << 23);
+    float shi[4] = {0.f, 0.f, 0.f, 0.f}, sr[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {  // output chunk c: columns 8c .. 8c + 7 of the hi and lo rows
+      uint32_t hw[4], lw[4];
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const float y0 = v[8 * c + 2 * e] * sc, y1 = v[8 * c + 2 * e + 1] * sc;
+        const float h0 = __fadd_rn(__fadd_rn(y0, kRound16), -kRound16);
+        const float h1 = __fadd_rn(__fadd_rn(y1, kRound16), -kRound16);
+        const float r0 = __fadd_rn(y0, -h0), r1 = __fadd_rn(y1, -h1);
+        shi[e] = __fadd_rn(shi[e], __fadd_rn(h0, h1));
+        sr[e] = __fadd_rn(sr[e], __fadd_rn(r0, r1));
+        const __half2 hh = __floats2half2_rn(h0, h1), ll = __floats2half2_rn(r0, r1);
+        hw[e] = *reinterpret_cast<const uint32_t*>(&hh);
+        lw[e] = *reinterpret_cast<const uint32_t*>(&ll);
+      }
+      const uint32_t off = swz(row * 128 + c * 16, 128);
+      *reinterpret_cast<uint4*>(X0 + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+      *reinterpret_cast<uint4*>(X1 + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+    }
+    const float th = __fadd_rn(__fadd_rn(shi[0], shi[1]), __fadd_rn(shi[2], shi[3]));  // exact
+    const float tr = __fadd_rn(__fadd_rn(sr[0], sr[1]), __fadd_rn(sr[2], sr[3]));
+    const float rsc = __uint_as_float((uint32_t)(127 - k) << 23);  // 2^-k
+    const double tot = ((double)th + (double)tr) * (double)rsc;
+    rs_out[row] = rsc;
+    rt_out[row] = tot;
+    if (sums && row < vrows && row >= r_lo) acc += tot;
   }
-  acc += c0 + c1;
   fence_proxy_async_smem();  // generic-proxy writes -> tcgen05 operand reads
   __syncwarp();
 }
@@ -290,10 +339,52 @@ __device__ __forceinline__ void sum_split_rows(const uint8_t* X0, int term_bytes
   }
 }
 
+// Sum of rows [row_lo, row_hi) of an int8 / fp16 stage (K blocks of SW-byte
+// rows, 128 rows each) by one warp: int8 exactly with dp4a, fp16 in FP32
+// chains of at most 64 values per lane (the caller adds each stage's partial
+// to an FP64 aggregate).  Four 16-byte loads in flight per lane.
+template <typename InT, int W>
+__device__ __forceinline__ void sum_stage_rows(const uint8_t* stage, int row_lo, int row_hi, int& acci,
+                                               float& accf) {
+  using C = ScanCfg<InT, W>;
+  constexpr int CPR = C::SW / 16;  // 16-byte chunks per row of one K block
+  const int lane = threadIdx.x & 31;
+  float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
+  auto add = [&](const uint4 w, float& sa, float& sb) {
+    if constexpr (C::IS_INT) {
+      acci = __dp4a((int)w.x, 0x01010101, acci);
+      acci = __dp4a((int)w.y, 0x01010101, acci);
+      acci = __dp4a((int)w.z, 0x01010101, acci);
+      acci = __dp4a((int)w.w, 0x01010101, acci);
+    } else {
+      const __half2* h = reinterpret_cast<const __half2*>(&w);
+      const float2 f0 = __half22float2(h[0]), f1 = __half22float2(h[1]);
+      const float2 f2 = __half22float2(h[2]), f3 = __half22float2(h[3]);
+      sa += (f0.x + f0.y) + (f1.x + f1.y);
+      sb += (f2.x + f2.y) + (f3.x + f3.y);
+    }
+  };
+  const int v1 = row_hi * CPR;
+#pragma unroll
+  for (int kb = 0; kb < C::KB; ++kb) {
+    const uint4* src = reinterpret_cast<const uint4*>(stage + kb * (128 * C::SW));
+    int v = row_lo * CPR + lane;
+    for (; v + 96 < v1; v += 128) {
+      const uint4 w0 = src[v], w1 = src[v + 32], w2 = src[v + 64], w3 = src[v + 96];
+      add(w0, s0, s1);
+      add(w1, s2, s3);
+      add(w2, s0, s1);
+      add(w3, s2, s3);
+    }
+    for (; v < v1; v += 32) add(src[v], s0, s1);
+  }
+  if constexpr (!C::IS_INT) accf += (s0 + s1) + (s2 + s3);
+}
+
 template <typename InT>
 struct OperandT { using T = InT; };
 template <>
-struct OperandT<float> { using T = __nv_bfloat16; };
+struct OperandT<float> { using T = __half; };
 template <>
 struct OperandT<SplitF32> { using T = __nv_bfloat16; };
 
@@ -353,7 +444,7 @@ template <typename InT, int W, int MODE>
 __device__ __forceinline__ void scan_epilogue(const ScanParams& p, const CUtensorMap& out_map, uint8_t* smem,
                                               ScanCtrl* ctl, uint32_t tmem_base, uint32_t epoch,
                                               const WaitCtx& wc) {
-  using C = ScanCfg<InT, W>;
+  using C = ScanCfg<InT, W, false, MODE == kScanFullSmall>;
   constexpr bool IS_INT = C::IS_INT;
   constexpr int BPT = C::BPT;
   using V = typename std::conditional<IS_INT, long long, double>::type;
@@ -367,6 +458,9 @@ __device__ __forceinline__ void scan_epilogue(const ScanParams& p, const CUtenso
   uint8_t* stg_base = smem + C::OFF_STG + g * C::STG_BUFS * C::STG_BYTES;
   const V start = scan_start<V, IS_INT>(p);
   uint32_t nfill = 0;
+  // F16SPLIT: this warpgroup's row totals and row scale factors
+  const double* rtg = reinterpret_cast<const double*>(smem + C::OFF_RT) + g * BPT * 128;
+  const float* rsg = reinterpret_cast<const float*>(smem + C::OFF_RS) + g * BPT * 128;
 
   const bool prof = p.phase_ns != nullptr && wg_thread == 0;
   uint64_t t_mark = prof ? globaltimer() : 0;
@@ -393,9 +487,11 @@ __device__ __forceinline__ void scan_epilogue(const ScanParams& p, const CUtenso
     for (int j = 0; j < BPT; ++j) rowex[j] = V(0);
     if constexpr (MODE != kScanRows) {
       uint32_t tb[BPT];
+      if constexpr (!C::F16SPLIT) {
 #pragma unroll
-      for (int j = 0; j < BPT; ++j) tb[j] = tmem_ld1(tm + (uint32_t)(j * W + W - 1));
-      tmem_wait_ld();
+        for (int j = 0; j < BPT; ++j) tb[j] = tmem_ld1(tm + (uint32_t)(j * W + W - 1));
+        tmem_wait_ld();
+      }
       int fl[BPT];
 #pragma unroll
       for (int j = 0; j < BPT; ++j) {
@@ -417,6 +513,9 @@ __device__ __forceinline__ void scan_epilogue(const ScanParams& p, const CUtenso
 #pragma unroll
       for (int j = 0; j < BPT; ++j) {
         V ti = IS_INT ? (V)(int)tb[j] : (V)__uint_as_float(tb[j]);
+        if constexpr (C::F16SPLIT) {  // the exact row totals of the converters
+          if (row_tile0 + j * 128 + r < p.full_rows) ti = (V)rtg[j * 128 + r];
+        }
         int fi = fl[j];
 #pragma unroll
         for (int d = 1; d < 32; d <<= 1) {
@@ -456,7 +555,7 @@ __device__ __forceinline__ void scan_epilogue(const ScanParams& p, const CUtenso
         if (bf) { run = bsum; runf = 1; } else { run += bsum; }
       }
       if (prof) { const uint64_t t = globaltimer(); phase_add(p, 1, t - t_mark); t_mark = t; }
-      if constexpr (MODE == kScanFull) {
+      if constexpr (is_full(MODE)) {
         // The summer warp published this tile's aggregate as soon as its data
         // landed; wait for that (ordering: the inclusive prefix must not be
         // overwritten by a late aggregate), then look back.
@@ -479,6 +578,7 @@ __device__ __forceinline__ void scan_epilogue(const ScanParams& p, const CUtenso
       int acci = 0;
       const float cf = IS_INT ? 0.f : (float)rowex[j];
       const uint32_t ci = IS_INT ? (uint32_t)(long long)rowex[j] : 0u;
+      const float rsv = C::F16SPLIT ? rsg[j * 128 + r] : 1.f;  // read before block j's slot is released
 #pragma unroll
       for (int h = 0; h < C::NFILL; ++h) {
         uint8_t* stg = stg_base + (nfill % C::STG_BUFS) * C::STG_BYTES;
@@ -491,6 +591,10 @@ __device__ __forceinline__ void scan_epilogue(const ScanParams& p, const CUtenso
         for (int c = 0; c < C::FILLW / 16; ++c)
           tmem_ld16(tm + (uint32_t)(j * W + h * C::FILLW + c * 16), *reinterpret_cast<uint32_t(*)[16]>(&v[c * 16]));
         tmem_wait_ld();
+        if constexpr (C::F16SPLIT) {  // undo the row's operand scale (a power of two: exact)
+#pragma unroll
+          for (int c = 0; c < C::FILLW; ++c) v[c] = __float_as_uint(__uint_as_float(v[c]) * rsv);
+        }
         if (h == C::NFILL - 1) {
           tc_fence_before();
           __syncwarp();
@@ -654,7 +758,7 @@ __device__ __forceinline__ void ctl_publish_seg(const ScanParams& p, uint32_t ti
 template <typename InT, int W, int MODE>
 __device__ __forceinline__ void scan_summer(const ScanParams& p, uint8_t* smem, ScanCtrl* ctl, uint32_t epoch,
                                                 const WaitCtx& wc) {
-  using C = ScanCfg<InT, W, is_seg(MODE)>;
+  using C = ScanCfg<InT, W, is_seg(MODE), MODE == kScanFullSmall>;
   constexpr bool IS_INT = C::IS_INT;
   constexpr int BPT = C::BPT;
   using V = typename std::conditional<IS_INT, long long, double>::type;
@@ -667,7 +771,7 @@ __device__ __forceinline__ void scan_summer(const ScanParams& p, uint8_t* smem, 
   // latter the aggregate is the sum after that start, flagged as a segment
   // start, which ends every look-back that reaches the tile.
   constexpr bool SEG_EARLY = (MODE == kSegBounds || MODE == kSegPeriodic);
-  constexpr bool SUMS = (MODE == kScanFull || SEG_EARLY);
+  constexpr bool SUMS = (is_full(MODE) || SEG_EARLY);
   uint32_t k = 0;
   uint32_t i = 0;
   for (;; ++i) {
@@ -722,13 +826,24 @@ __device__ __forceinline__ void scan_summer(const ScanParams& p, uint8_t* smem, 
         const int64_t row0 = ((int64_t)tid * BPT + j) * 128;
         const int64_t vr = p.full_rows - row0;
         const int vrows = vr <= 0 ? 0 : (vr >= 128 ? 128 : (int)vr);
-        float acc = 0.f;  // this stage's partial (FP32), then the FP64 tile aggregate
         if constexpr (C::PRESPLIT) {
+          float acc = 0.f;  // this stage's partial (FP32), then the FP64 tile aggregate
           if (SUMS) sum_split_rows(X0, C::TERM_BYTES, 0, 16, r_lo, vrows, acc);
+          accd += (double)acc;
         } else {
-          convert_f32_rows(X0, C::TERM_BYTES, 0, 16, r_lo, vrows, SUMS, acc);
+          // the row scales / totals of this TMEM half are free once the
+          // epilogue has drained block j of the tile two before this one
+          const int g = i & 1;
+          const uint32_t u = i >> 1;
+          if (u >= 1 && !__all_sync(0xffffffffu, mbar_wait(&ctl->slot_empty[g][j], (u & 1u) ^ 1u, wc, 11, i))) {
+            stop = true;
+            break;
+          }
+          const int rix = (g * BPT + j) * 128;
+          convert_f32_rows(X0, C::TERM_BYTES, 0, 64, r_lo, vrows, SUMS, accd,
+                           reinterpret_cast<float*>(smem + C::OFF_RS) + rix,
+                           reinterpret_cast<double*>(smem + C::OFF_RT) + rix);
         }
-        accd += (double)acc;
         if (lane == 0) mbar_arrive(&ctl->conv[s]);
         if constexpr (SUMS) {  // the other half's sum, stored before its conv arrival
           const bool okc = __all_sync(0xffffffffu, mbar_wait(&ctl->conv[s], (k / C::NSTAGE) & 1u, wc, 9, i));
@@ -737,34 +852,25 @@ __device__ __forceinline__ void scan_summer(const ScanParams& p, uint8_t* smem, 
         }
       }
       if constexpr (SUMS && !C::IS_F32) {
+        // int8: the whole stage here (dp4a is cheap); fp16: rows [r_lo, 64)
+        // here and rows [64, 128) by warp 11, which leaves its partial in
+        // cv_sum[s] before its conv arrival -- the stage is released only
+        // after both halves have been read
         const int64_t row0 = ((int64_t)tid * BPT + j) * 128;
         int64_t vr = p.full_rows - row0;
         const int vrows = vr <= 0 ? 0 : (vr >= 128 ? 128 : (int)vr);
-        const int nv = vrows * (C::SW / 16);
-        // fp16: a stage's values are summed in FP32 in two independent
-        // chains (at most 64 values each per lane) and each stage's partial
-        // goes to the FP64 tile aggregate, which feeds carries across tiles
-        float s0 = 0.f, s1 = 0.f;
-#pragma unroll
-        for (int kb = 0; kb < C::KB; ++kb) {
-          const uint4* src = (const uint4*)(smem + s * C::STAGE_BYTES + kb * (128 * C::SW));
-          for (int v = r_lo * (C::SW / 16) + lane; v < nv; v += 32) {
-            const uint4 w = src[v];
-            if constexpr (IS_INT) {
-              acci = __dp4a((int)w.x, 0x01010101, acci);
-              acci = __dp4a((int)w.y, 0x01010101, acci);
-              acci = __dp4a((int)w.z, 0x01010101, acci);
-              acci = __dp4a((int)w.w, 0x01010101, acci);
-            } else {
-              const __half2* h = reinterpret_cast<const __half2*>(&w);
-              const float2 f0 = __half22float2(h[0]), f1 = __half22float2(h[1]);
-              const float2 f2 = __half22float2(h[2]), f3 = __half22float2(h[3]);
-              s0 += (f0.x + f0.y) + (f1.x + f1.y);
-              s1 += (f2.x + f2.y) + (f3.x + f3.y);
-            }
-          }
+        float sf = 0.f;
+        if constexpr (IS_INT) {
+          sum_stage_rows<InT, W>(smem + s * C::STAGE_BYTES, r_lo, vrows, acci, sf);
+        } else {
+          sum_stage_rows<InT, W>(smem + s * C::STAGE_BYTES, r_lo, vrows < 64 ? vrows : 64, acci, sf);
+          accd += (double)sf;
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&ctl->conv[s]);
+          const bool okc = __all_sync(0xffffffffu, mbar_wait(&ctl->conv[s], (k / C::NSTAGE) & 1u, wc, 13, i));
+          if (!okc) { stop = true; break; }
+          if (lane == 0) accd += ctl->cv_sum[s];
         }
-        if constexpr (!IS_INT) accd += (double)(s0 + s1);
       }
       __syncwarp();
       if (lane == 0) mbar_arrive(&ctl->empty[s]);  // this consumer is done with the stage
@@ -807,7 +913,7 @@ __device__ __forceinline__ void scan_summer(const ScanParams& p, uint8_t* smem, 
       if (prof) phase_add(p, 5, globaltimer() - t0);
       if (!ok) break;
     }
-    if constexpr (MODE == kScanFull) {
+    if constexpr (is_full(MODE)) {
       const int64_t tile_row0 = (int64_t)tid * BPT * 128;
       if (lane == 0 && p.tail > 0 && p.full_rows >= tile_row0 && p.full_rows < tile_row0 + BPT * 128) {
         float af = 0.f;
@@ -835,17 +941,54 @@ __device__ __forceinline__ void scan_summer(const ScanParams& p, uint8_t* smem, 
   }
 }
 
-// Second converter warp of fp32 launches: splits rows 64-127 of every stage
-// and leaves their sum (rows after the tile's last segment start, for the
-// modes whose aggregate the summer publishes) in cv_sum[s] before its conv
-// arrival.  Idle for the other input types.
+// Second converter warp: for fp32 launches it splits rows 64-127 of every
+// stage; for fp16 launches whose tile aggregate the summer publishes it sums
+// rows 64-127.  Either way it leaves the sum of its rows (those after the
+// tile's last segment start, for the modes whose aggregate the summer
+// publishes) in cv_sum[s] before its conv arrival.  Idle otherwise.
 template <typename InT, int W, int MODE>
 __device__ __forceinline__ void scan_converter2(const ScanParams& p, uint8_t* smem, ScanCtrl* ctl,
                                                 const WaitCtx& wc) {
-  using C = ScanCfg<InT, W, is_seg(MODE)>;
+  using C = ScanCfg<InT, W, is_seg(MODE), MODE == kScanFullSmall>;
+  constexpr bool SUMS_ANY = (is_full(MODE) || MODE == kSegBounds || MODE == kSegPeriodic);
+  if constexpr (!C::IS_F32 && !C::IS_INT && SUMS_ANY) {
+    constexpr int BPT = C::BPT;
+    constexpr bool SEG_EARLY = (MODE == kSegBounds || MODE == kSegPeriodic);
+    const int lane = threadIdx.x & 31;
+    uint32_t k = 0;
+    for (uint32_t i = 0;; ++i) {
+      long long ls = -1;
+      bool stop = false;
+      for (int j = 0; j < BPT; ++j, ++k) {
+        const int s = k % C::NSTAGE;
+        const bool ok = __all_sync(0xffffffffu, mbar_wait(&ctl->full[s], (k / C::NSTAGE) & 1u, wc, 14, i));
+        if (!ok) { stop = true; break; }
+        const uint32_t tid = *(volatile uint32_t*)&ctl->stage_cid[s];
+        if (tid == kSentinel) { stop = true; break; }
+        if (SEG_EARLY && j == 0) ls = tile_last_start<MODE>(p, tid, C::TILE_ELEMS);
+        int r_lo = 0;
+        if (SEG_EARLY && ls >= 0) {
+          const int64_t be0 = (int64_t)tid * C::TILE_ELEMS + (int64_t)j * 128 * W;
+          if (ls >= be0 + 128 * (int64_t)W) r_lo = 128;
+          else if (ls >= be0) r_lo = (int)((ls - be0) / W) + 1;
+        }
+        const int64_t row0 = ((int64_t)tid * BPT + j) * 128;
+        const int64_t vr = p.full_rows - row0;
+        const int vrows = vr <= 0 ? 0 : (vr >= 128 ? 128 : (int)vr);
+        int acci = 0;
+        float accf = 0.f;
+        sum_stage_rows<InT, W>(smem + s * C::STAGE_BYTES, r_lo > 64 ? r_lo : 64, vrows, acci, accf);
+        const double t = warp_sum_any((double)accf);
+        if (lane == 0) ctl->cv_sum[s] = t;
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&ctl->conv[s]);
+      }
+      if (stop) break;
+    }
+  }
   if constexpr (C::IS_F32) {
     constexpr int BPT = C::BPT;
-    constexpr bool SUMS = (MODE == kScanFull || MODE == kSegBounds || MODE == kSegPeriodic);
+    constexpr bool SUMS = (is_full(MODE) || MODE == kSegBounds || MODE == kSegPeriodic);
     const int lane = threadIdx.x & 31;
     uint32_t k = 0;
     for (uint32_t i = 0;; ++i) {
@@ -871,14 +1014,26 @@ __device__ __forceinline__ void scan_converter2(const ScanParams& p, uint8_t* sm
         const int64_t row0 = ((int64_t)tid * BPT + j) * 128;
         const int64_t vr = p.full_rows - row0;
         const int vrows = vr <= 0 ? 0 : (vr >= 128 ? 128 : (int)vr);
-        float acc = 0.f;
+        double acc = 0.0;
         if constexpr (C::PRESPLIT) {
-          if (SUMS) sum_split_rows(smem + s * C::STAGE_BYTES, C::TERM_BYTES, 16, 32, r_lo, vrows, acc);
+          float accf = 0.f;
+          if (SUMS) sum_split_rows(smem + s * C::STAGE_BYTES, C::TERM_BYTES, 16, 32, r_lo, vrows, accf);
+          acc = (double)accf;
         } else {
-          convert_f32_rows(smem + s * C::STAGE_BYTES, C::TERM_BYTES, 16, 32, r_lo, vrows, SUMS, acc);
+          const int g = i & 1;
+          const uint32_t u = i >> 1;
+          if (u >= 1 && !__all_sync(0xffffffffu, mbar_wait(&ctl->slot_empty[g][j], (u & 1u) ^ 1u, wc, 12, i))) {
+            if (lane == 0) mbar_arrive(&ctl->conv[s]);
+            stop = true;
+            break;
+          }
+          const int rix = (g * BPT + j) * 128;
+          convert_f32_rows(smem + s * C::STAGE_BYTES, C::TERM_BYTES, 64, 128, r_lo, vrows, SUMS, acc,
+                           reinterpret_cast<float*>(smem + C::OFF_RS) + rix,
+                           reinterpret_cast<double*>(smem + C::OFF_RT) + rix);
         }
         if constexpr (SUMS) {
-          const double t = warp_sum_any((double)acc);
+          const double t = warp_sum_any(acc);
           if (lane == 0) ctl->cv_sum[s] = t;
         }
         __syncwarp();
@@ -961,6 +1116,9 @@ __device__ __forceinline__ void seg_epilogue(const ScanParams& p, const CUtensor
   unsigned long long* smask = reinterpret_cast<unsigned long long*>(smem + C::OFF_MASK) + g * BPT * 128;
   int* votes = ctl->wg_vote[g];
   const bool sums_out = (MODE == kSegBounds) && p.out_sums;
+  // F16SPLIT: this warpgroup's row totals and row scale factors
+  const double* rtg = reinterpret_cast<const double*>(smem + C::OFF_RT) + g * BPT * 128;
+  const float* rsg = reinterpret_cast<const float*>(smem + C::OFF_RS) + g * BPT * 128;
   const bool prof = p.phase_ns != nullptr && wg_thread == 0;
   uint64_t t_mark = prof ? globaltimer() : 0;
   uint32_t nfill = 0;
@@ -1026,6 +1184,7 @@ __device__ __forceinline__ void seg_epilogue(const ScanParams& p, const CUtensor
     int exf[BPT];
     {
       uint32_t tb[BPT];
+      double tbd[BPT];  // F16SPLIT: row aggregates in FP64 (exact totals for rows without a start)
       int fl[BPT];
 #pragma unroll
       for (int j = 0; j < BPT; ++j) {
@@ -1036,16 +1195,23 @@ __device__ __forceinline__ void seg_epilogue(const ScanParams& p, const CUtensor
         // row aggregate after the row's last segment start: z[W-1] - z[ls-1]
         // (z[W-1] alone when the row holds no start).  Rows of a warp with
         // no start and no ragged tail need only their last column.
-        uint32_t last, base = 0u;
+        uint32_t last = 0u, base = 0u;
         if (!__any_sync(0xffffffffu, mk != 0ull || is_tail)) {
-          last = tmem_ld1(tm + (uint32_t)(j * W + W - 1));
-          tmem_wait_ld();
+          if constexpr (!C::F16SPLIT) {
+            last = tmem_ld1(tm + (uint32_t)(j * W + W - 1));
+            tmem_wait_ld();
+          }
         } else {
           uint32_t v[W];
 #pragma unroll
           for (int c = 0; c < W / 16; ++c)
             tmem_ld16(tm + (uint32_t)(j * W + c * 16), *reinterpret_cast<uint32_t(*)[16]>(&v[c * 16]));
           tmem_wait_ld();
+          if constexpr (C::F16SPLIT) {
+            const float rsv = rsg[j * 128 + r];
+#pragma unroll
+            for (int c = 0; c < W; ++c) v[c] = __float_as_uint(__uint_as_float(v[c]) * rsv);
+          }
           if (is_tail) {
             float accf = 0.f;
             int acci = 0;
@@ -1084,12 +1250,15 @@ __device__ __forceinline__ void seg_epilogue(const ScanParams& p, const CUtensor
         const bool seen = mk != 0ull;
         if constexpr (IS_INT) tb[j] = live ? (uint32_t)((int)last - (seen ? (int)base : 0)) : 0u;
         else tb[j] = live ? __float_as_uint(__uint_as_float(last) - (seen ? __uint_as_float(base) : 0.f)) : 0u;
+        if constexpr (C::F16SPLIT)  // the exact row total when the aggregate is the whole row (no start after column 0)
+          tbd[j] = (live && mk <= 1ull && !is_tail) ? rtg[j * 128 + r] : (double)__uint_as_float(tb[j]);
         fl[j] = (live && mk != 0ull) ? 1 : 0;
       }
       int rowf[BPT];
 #pragma unroll
       for (int j = 0; j < BPT; ++j) {
         V ti = IS_INT ? (V)(int)tb[j] : (V)__uint_as_float(tb[j]);
+        if constexpr (C::F16SPLIT) ti = (V)tbd[j];
         int fi = fl[j];
 #pragma unroll
         for (int d = 1; d < 32; d <<= 1) {
@@ -1155,6 +1324,7 @@ __device__ __forceinline__ void seg_epilogue(const ScanParams& p, const CUtensor
       int acci = 0;
       const float cf = IS_INT ? 0.f : (float)rowex[j];
       const uint32_t ci = IS_INT ? (uint32_t)(long long)rowex[j] : 0u;
+      const float rsv = C::F16SPLIT ? rsg[j * 128 + r] : 1.f;  // read before block j's slot is released
       uint8_t* stg = stg_base + (nfill % C::STG_BUFS) * C::STG_BYTES;
       // per-segment sums: the first chunk of this block's bounds is loaded
       // now, its latency hidden behind the row work below
@@ -1176,6 +1346,10 @@ __device__ __forceinline__ void seg_epilogue(const ScanParams& p, const CUtensor
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(&ctl->slot_empty[g][j]);
+      if constexpr (C::F16SPLIT) {  // undo the row's operand scale (a power of two: exact)
+#pragma unroll
+        for (int c = 0; c < W; ++c) v[c] = __float_as_uint(__uint_as_float(v[c]) * rsv);
+      }
       if (is_tail) {
 #pragma unroll
         for (int c = 0; c < W / 16; ++c)
@@ -1285,7 +1459,7 @@ template <typename InT, int W, int MODE>
 __global__ void __launch_bounds__(kThreads, 1)
     scan_tc_kernel(const __grid_constant__ CUtensorMap in_map, const __grid_constant__ CUtensorMap out_map,
                    const ScanParams p) {
-  using C = ScanCfg<InT, W, is_seg(MODE)>;
+  using C = ScanCfg<InT, W, is_seg(MODE), MODE == kScanFullSmall>;
   constexpr bool IS_INT = C::IS_INT;
   constexpr int BPT = C::BPT;
   using V = typename std::conditional<IS_INT, long long, double>::type;
@@ -1385,7 +1559,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     if (lane == 0) {
       constexpr uint32_t IDESC =
           IS_INT ? umma_idesc(CF_S32, AB_S8, 128, W)
-                 : umma_idesc(CF_F32, (__is_same(InT, __nv_bfloat16) || C::IS_F32) ? AB_BF16 : AB_F16, 128, W);
+                 : umma_idesc(CF_F32, (__is_same(InT, __nv_bfloat16) || C::PRESPLIT) ? AB_BF16 : AB_F16, 128, W);
       const uint32_t b_addr = smem_u32(bmat);
       uint32_t k = 0;
       for (uint32_t i = 0;; ++i) {  // tile sequence of this CTA

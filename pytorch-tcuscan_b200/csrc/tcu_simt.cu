@@ -402,6 +402,102 @@ static tcu_status_t launched(const char* what) {
   return e == cudaSuccess ? TCU_OK : cuda_fail(e, what);
 }
 
+// ---------------------------------------------------------------------------
+// total: the sum of all n elements in a wide type -- int8 -> int64 (exact),
+// fp16 / fp32 -> FP64 -- in a fixed order, so every call gives the same bits:
+// block b sums 16-byte chunks b*256 + t, b*256 + t + grid*256, ... per thread
+// (int8 chunks exactly with dp4a, fp16 / fp32 chunks in FP64), then a fixed
+// warp / block tree; one block adds the block partials in a fixed tree and
+// zeroes them (workspace scratch).  The exchange step of the sharded scan.
+template <typename InT>
+struct TotalAcc { using T = double; };
+template <>
+struct TotalAcc<int8_t> { using T = long long; };
+
+template <typename InT>
+__device__ __forceinline__ typename TotalAcc<InT>::T chunk_total(const uint4 w) {
+  if constexpr (__is_same(InT, int8_t)) {
+    int s = __dp4a((int)w.x, 0x01010101, 0);
+    s = __dp4a((int)w.y, 0x01010101, s);
+    s = __dp4a((int)w.z, 0x01010101, s);
+    s = __dp4a((int)w.w, 0x01010101, s);
+    return (long long)s;
+  } else if constexpr (__is_same(InT, __half)) {
+    const __half2* h = reinterpret_cast<const __half2*>(&w);
+    double t = 0.0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const float2 f = __half22float2(h[k]);
+      t += (double)f.x + (double)f.y;
+    }
+    return t;
+  } else {
+    return ((double)__uint_as_float(w.x) + (double)__uint_as_float(w.y)) +
+           ((double)__uint_as_float(w.z) + (double)__uint_as_float(w.w));
+  }
+}
+
+template <typename InT>
+__global__ void __launch_bounds__(256) total_partial_kernel(const InT* __restrict__ x, int64_t n,
+                                                            typename TotalAcc<InT>::T* __restrict__ part) {
+  using A = typename TotalAcc<InT>::T;
+  constexpr int VPC = 16 / (int)sizeof(InT);  // elements per 16-byte chunk
+  const int64_t nchunks = n / VPC;
+  const uint4* xv = reinterpret_cast<const uint4*>(x);
+  A acc = 0;
+  for (int64_t c = (int64_t)blockIdx.x * 256 + threadIdx.x; c < nchunks; c += (int64_t)gridDim.x * 256)
+    acc += chunk_total<InT>(__ldg(xv + c));
+  if (blockIdx.x == 0) {  // the elements after the last whole chunk
+    for (int64_t i = nchunks * VPC + threadIdx.x; i < n; i += 256) {
+      if constexpr (__is_same(InT, int8_t)) acc += (long long)x[i];
+      else if constexpr (__is_same(InT, __half)) acc += (double)__half2float(x[i]);
+      else acc += (double)x[i];
+    }
+  }
+  acc = warp_sum_any(acc);
+  __shared__ A sw[8];
+  if ((threadIdx.x & 31) == 0) sw[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    A t = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) t += sw[k];
+    part[blockIdx.x] = t;
+  }
+}
+
+template <typename A>
+__global__ void __launch_bounds__(256) total_final_kernel(A* __restrict__ part, int nparts, A* __restrict__ out) {
+  A acc = 0;
+  for (int k = threadIdx.x; k < nparts; k += 256) acc += part[k];
+  acc = warp_sum_any(acc);
+  __shared__ A sw[8];
+  if ((threadIdx.x & 31) == 0) sw[threadIdx.x >> 5] = acc;
+  __syncthreads();  // every partial has been read
+  for (int k = threadIdx.x; k < nparts; k += 256) part[k] = 0;
+  if (threadIdx.x == 0) {
+    A t = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) t += sw[k];
+    *out = t;
+  }
+}
+
+template <typename InT>
+static tcu_status_t run_total(const void* x, int64_t n, void* out, void* ws, size_t ws_bytes, cudaStream_t st) {
+  using A = typename TotalAcc<InT>::T;
+  constexpr int VPC = 16 / (int)sizeof(InT);
+  int64_t grid = (n / VPC + 255) / 256;
+  const int64_t cap = (int64_t)sm_count() * 4;
+  grid = grid < 1 ? 1 : (grid > cap ? cap : grid);
+  if (!ws || ws_capacity(ws_bytes) * (int64_t)sizeof(TileDesc) < grid * (int64_t)sizeof(A)) return TCU_ERR_WORKSPACE;
+  A* part = reinterpret_cast<A*>(ws_descs(ws));  // zeroed again by the final kernel
+  total_partial_kernel<InT><<<(unsigned)grid, 256, 0, st>>>(static_cast<const InT*>(x), n, part);
+  total_final_kernel<A><<<1, 256, 0, st>>>(part, (int)grid, static_cast<A*>(out));
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? TCU_OK : cuda_fail(e, "total launch");
+}
+
 // Scratch written into a workspace's look-back descriptor region is zeroed
 // after use, so that the region only ever holds descriptors or zeros: stale
 // partial sums could otherwise read as a valid descriptor of a later launch
@@ -580,6 +676,25 @@ tcu_status_t tcu_complete_blocks(const void* x, tcu_dtype_t dtype, int64_t n, co
     return TCU_ERR_DTYPE;
   }
   return launched("complete_blocks");
+}
+
+tcu_status_t tcu_total(const void* x, tcu_dtype_t dtype, int64_t n, void* out, void* ws, size_t ws_bytes,
+                       void* stream) {
+  if (n < 0 || !out) return TCU_ERR_ARG;
+  if (reinterpret_cast<uintptr_t>(out) & 7u) return TCU_ERR_ALIGN;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (n == 0) {
+    cudaError_t e = cudaMemsetAsync(out, 0, 8, st);
+    return e == cudaSuccess ? TCU_OK : cuda_fail(e, "cudaMemsetAsync(total)");
+  }
+  if (!x) return TCU_ERR_ARG;
+  if (!aligned16(x)) return TCU_ERR_ALIGN;
+  switch (dtype) {
+    case TCU_INT8: return run_total<int8_t>(x, n, out, ws, ws_bytes, st);
+    case TCU_FLOAT16: return run_total<__half>(x, n, out, ws, ws_bytes, st);
+    case TCU_FLOAT32: return run_total<float>(x, n, out, ws, ws_bytes, st);
+    default: return TCU_ERR_DTYPE;
+  }
 }
 
 tcu_status_t tcu_gen_lower(int64_t s, tcu_dtype_t dtype, void* z, void* stream) {

@@ -70,10 +70,8 @@ def _scan(x, S, start, where):
     if n == 0:
         return z
     S = _pick_S(S, x.dtype, n)
-    ws, wsb = workspace(x.device, _lib.lib.tcu_workspace_bytes(n, S))
-    st = _lib.lib.tcu_scan(
-        x.data_ptr(), _lib.DTYPE_CODE[x.dtype], n, S, float(start), z.data_ptr(), ws, wsb, stream_ptr(x.device)
-    )
+    ws, wsb, sp = _lib.launch_context(x.device, _lib.lib.tcu_workspace_bytes(n, S))
+    st = _lib.lib.tcu_scan(x.data_ptr(), _lib.DTYPE_CODE[x.dtype], n, S, float(start), z.data_ptr(), ws, wsb, sp)
     check(st, where)
     _after(x)
     return z

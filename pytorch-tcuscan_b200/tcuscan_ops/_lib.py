@@ -66,10 +66,14 @@ _sig("tcu_set_phase_profile", None, _I)
 _sig("tcu_set_max_ctas", None, _I)
 _sig("tcu_selftest_wait_timeout", _ST, _I, _U64, _P, _SZ, _P)
 _sig("tcu_get_max_ctas", _I)
+_sig("tcu_set_small_tile_limit", None, _I)
+_sig("tcu_get_small_tile_limit", _I)
 _sig("tcu_workspace_phase_ns", _ST, _P, ctypes.POINTER(ctypes.c_uint64), _I, _P)
 _sig("tcu_scan", _ST, _P, _I, _I64, _I, _D, _P, _P, _SZ, _P)
 _sig("tcu_scan_cpu", _ST, _P, _I, _I64, _P, _I)
 _sig("tcu_scan_chained", _ST, _P, _I, _I64, _I, _D, _P, _P, _P, _SZ, _P)
+_sig("tcu_scan_chained_typed", _ST, _P, _I, _I64, _I, _D, _P, _I, _P, _P, _SZ, _P)
+_sig("tcu_total", _ST, _P, _I, _I64, _P, _P, _SZ, _P)
 _sig("tcu_row_scan", _ST, _P, _I, _I64, _I, _P, _P, _SZ, _P)
 _sig("tcu_block_scan", _ST, _P, _I, _I64, _I, _P, _P, _SZ, _P)
 _sig("tcu_seg_scan", _ST, _P, _I, _I64, _I, _P, _I, _P, _P, _SZ, _P)
@@ -124,11 +128,12 @@ def stream_ptr(device):
 
 
 class _Workspace:
-    __slots__ = ("buf", "bytes")
+    __slots__ = ("buf", "bytes", "ptr")
 
     def __init__(self):
         self.buf = None
         self.bytes = 0
+        self.ptr = None
 
 
 _ws_lock = threading.Lock()
@@ -143,7 +148,15 @@ def workspace(device, need_bytes):
     One workspace per stream keeps launches that may overlap on the GPU from
     sharing look-back state; launches on one stream are ordered, and each one
     leaves the workspace reset for the next (epoch-tagged flags)."""
-    dev = torch.device(device)
+    ws, wsb, _ = launch_context(device, need_bytes)
+    return ws, wsb
+
+
+def launch_context(device, need_bytes):
+    """(workspace ptr, workspace bytes, stream ptr) of (device, current
+    stream): one current-stream lookup for both (the per-call host cost of
+    the small scans is a few microseconds)."""
+    dev = device if isinstance(device, torch.device) else torch.device(device)
     stream = torch.cuda.current_stream(dev)
     key = (dev.index, stream.cuda_stream)
     with _ws_lock:
@@ -154,9 +167,12 @@ def workspace(device, need_bytes):
             nbytes = max(int(need_bytes), 1 << 20, 2 * ws.bytes)
             ws.buf = torch.empty(nbytes, dtype=torch.uint8, device=dev)
             ws.bytes = nbytes
+            ws.ptr = None
             check(lib.tcu_workspace_init(ctypes.c_void_p(ws.buf.data_ptr()), _SZ(nbytes),
                                          ctypes.c_void_p(stream.cuda_stream)), "tcu_workspace_init")
-        return ctypes.c_void_p(ws.buf.data_ptr()), _SZ(ws.bytes)
+        if ws.ptr is None:
+            ws.ptr = (ctypes.c_void_p(ws.buf.data_ptr()), _SZ(ws.bytes), ctypes.c_void_p(stream.cuda_stream))
+        return ws.ptr
 
 
 def workspace_error(device=None, clear=True):

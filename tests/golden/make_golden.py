@@ -2,7 +2,10 @@
 
 Run in the development container, where the reference checkout exists:
 
-    OMP_NUM_THREADS=4 python tests/golden/make_golden.py [--ref /root/reference]
+    OMP_NUM_THREADS=4 python tests/golden/make_golden.py [--ref /path/to/reference]
+
+(the checkout is found as in oracle/build_ref.py: --ref, $TCUSCAN_REFERENCE,
+or a ``reference`` directory next to this repository)
 
 Two sources of expected outputs, both the reference's own code:
 
@@ -54,7 +57,7 @@ def _extract(ref_root, test_file, names, extra_ns):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=None)
     args = ap.parse_args()
 
     import torch
@@ -63,6 +66,10 @@ def main():
 
     sys.path.insert(0, REPO)
     from oracle import build_ref
+
+    args.ref = build_ref.reference_root(args.ref)
+    if args.ref is None:
+        raise SystemExit("reference checkout not found (pass --ref or set TCUSCAN_REFERENCE)")
 
     # The reference oracles call .npu(); on CPU that is the identity.
     torch.Tensor.npu = lambda self, *a, **k: self

@@ -25,8 +25,8 @@ def _free_port():
 
 def _cpu_total(x):
     if x.dtype == torch.int8:
-        return x.to(torch.int64).sum().to(torch.int32).reshape(1)  # two's-complement wrap
-    return x.to(torch.float64).sum().to(torch.float32).reshape(1)
+        return x.to(torch.int64).sum().reshape(1)
+    return x.to(torch.float64).sum().reshape(1)
 
 
 def _cpu_scan(x, S, prefix):
@@ -85,12 +85,20 @@ def test_scan_sharded_host_logic_gloo(dtype_name, lengths):
         assert np.max(np.abs(z - ref) / np.maximum(np.abs(ref), 1.0)) <= 1e-6
 
 
-def test_exclusive_prefix_wraps_int32():
+def test_exclusive_prefix_wide_totals():
+    """Totals travel as int64 (int8 pieces) / float64 (float pieces): the
+    prefix of the ranks before does not wrap or round to fp32; the int32 wrap
+    happens only in the chained scan's output, as in the unsharded scan."""
     sys.path.insert(0, PKG)
     from tcuscan_b200 import dist as tdist
 
-    t = [torch.tensor([2 ** 31 - 1], dtype=torch.int32), torch.tensor([5], dtype=torch.int32),
-         torch.tensor([1], dtype=torch.int32)]
+    assert tdist.total_dtype(torch.int8) == torch.int64
+    assert tdist.total_dtype(torch.float16) == torch.float64 == tdist.total_dtype(torch.float32)
+    t = [torch.tensor([2 ** 31 - 1], dtype=torch.int64), torch.tensor([5], dtype=torch.int64),
+         torch.tensor([1], dtype=torch.int64)]
     assert int(tdist.exclusive_prefix(t, 0).item()) == 0
     assert int(tdist.exclusive_prefix(t, 1).item()) == 2 ** 31 - 1
-    assert int(tdist.exclusive_prefix(t, 2).item()) == -(2 ** 31) + 4
+    assert int(tdist.exclusive_prefix(t, 2).item()) == 2 ** 31 + 4
+    f = [torch.tensor([1.0 + 2 ** -40], dtype=torch.float64), torch.tensor([2 ** -40], dtype=torch.float64),
+         torch.tensor([0.5], dtype=torch.float64)]
+    assert float(tdist.exclusive_prefix(f, 2).item()) == 1.0 + 2 ** -39  # below fp32 resolution
