@@ -151,10 +151,17 @@ TCU_API tcu_status_t tcu_total(const void* x, tcu_dtype_t dtype, int64_t n, void
  * device after cudaDeviceReset has been called on it.  All calls share the
  * array and it keeps the last call's contents, so calls that can overlap on
  * the GPU (other streams, other threads) race -- serialise them.
- * Device-side wait timeouts are not reported by this variant (tcu_scan with
- * a workspace reports them through tcu_workspace_error).                   */
+ * A device-side wait that ran out leaves its error in the shared array (each
+ * call clears it first); read it with tcu_scan_noalloc_error after the call
+ * and before the next one on that device.                                  */
 TCU_API tcu_status_t tcu_scan_noalloc(const void* x, tcu_dtype_t x_dtype, int64_t n, int S, double start, void* z,
                                       void* stream);
+/* Error words of the last tcu_scan_noalloc call on the current device:
+ * synchronises `stream`, copies them into info (info[0] = status code,
+ * info[1] = site, info[2] = chunk; all zero when the call succeeded) with no
+ * allocation, clears them when clear != 0, and returns info[0].  No
+ * counterpart in the reference.                                            */
+TCU_API tcu_status_t tcu_scan_noalloc_error(uint32_t info[3], int clear, void* stream);
 
 /* Host-side inclusive scan of a host array (x and z in host memory; no GPU
  * work): int8 -> int32 (two's-complement wrap), fp16 / fp32 -> fp32.  The

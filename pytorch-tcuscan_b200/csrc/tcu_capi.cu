@@ -585,3 +585,30 @@ extern "C" tcu_status_t tcu_scan_noalloc(const void* x, tcu_dtype_t x_dtype, int
   if (x_dtype == TCU_INT8 && S == 16) S = 32;
   return dispatch_scan<kScanFull>(x, x_dtype, n, S, z, start, 0, ws, kNoAllocScratchBytes, st);
 }
+
+// The device-side error words of the last tcu_scan_noalloc call on the
+// current device (a bounded wait that ran out): synchronises `stream`, copies
+// the words out with one cudaMemcpyAsync into the caller's array (no
+// allocation) and optionally clears them.  A device that has not run the
+// scan yet reports TCU_OK.
+extern "C" tcu_status_t tcu_scan_noalloc_error(uint32_t info[3], int clear, void* stream) {
+  if (!info) return TCU_ERR_ARG;
+  info[0] = info[1] = info[2] = 0;
+  cudaStream_t st = (cudaStream_t)stream;
+  void* ws = nullptr;
+  tcu_status_t s = noalloc_scratch(st, &ws);
+  if (s != TCU_OK) return s;
+  uint32_t h[3];
+  cudaError_t e = cudaMemcpyAsync(h, &static_cast<WsHeader*>(ws)->error, sizeof(h), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_fail(e, "tcu_scan_noalloc_error: reading the scratch header");
+  info[0] = h[0];
+  info[1] = h[1];
+  info[2] = h[2];
+  if (clear && h[0]) {
+    e = cudaMemsetAsync(&static_cast<WsHeader*>(ws)->error, 0, sizeof(h), st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_fail(e, "tcu_scan_noalloc_error: clearing");
+  }
+  return (tcu_status_t)h[0];
+}

@@ -158,52 +158,59 @@ __global__ void __launch_bounds__(kNzThreads, 4) nz_split_kernel(const VT* __res
   float p[SPMV ? ITEMS : 1];
   uint32_t raw[WORDS];
   if constexpr (SPMV) {
-    int32_t cc[ITEMS];
-    float va[ITEMS];
-    if (full && ((reinterpret_cast<uintptr_t>(cols + j0) & 15u) == 0)) {
+    // Coalesced: lane L of warp w loads elements w*512 + q*128 + 4L .. +3
+    // (q = 0..3), so every load instruction covers whole 128-byte lines; the
+    // products then go through padded shared memory (16 bytes of padding per
+    // 32 products: conflict-free both ways) into each thread's 16
+    // consecutive elements, the order the row logic below needs.
+    static_assert(ITEMS == 16, "the SpMV transpose assumes 16 elements per thread");
+    __shared__ __align__(16) float s_prod[kNzWarps][512 + 64];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int64_t wbase = t_lo + (int64_t)w * 512;
+    const bool aligned = ((reinterpret_cast<uintptr_t>(cols) | reinterpret_cast<uintptr_t>(vals)) & 15u) == 0 &&
+                         (sizeof(VT) == 4 || (reinterpret_cast<uintptr_t>(vals) & 7u) == 0);
 #pragma unroll
-      for (int q = 0; q < ITEMS / 4; ++q) {
-        const int4 v4 = __ldg(reinterpret_cast<const int4*>(cols + j0) + q);
-        cc[4 * q] = v4.x;
-        cc[4 * q + 1] = v4.y;
-        cc[4 * q + 2] = v4.z;
-        cc[4 * q + 3] = v4.w;
-      }
-    } else {
+    for (int q = 0; q < 4; ++q) {
+      const int64_t e0 = wbase + q * 128 + 4 * lane;
+      int32_t cc[4];
+      float va[4];
+      if (aligned && e0 + 4 <= t_hi) {
+        const int4 c4 = __ldg(reinterpret_cast<const int4*>(cols + e0));
+        cc[0] = c4.x; cc[1] = c4.y; cc[2] = c4.z; cc[3] = c4.w;
+        if constexpr (sizeof(VT) == 4) {
+          const float4 v4 = __ldg(reinterpret_cast<const float4*>(vals + e0));
+          va[0] = v4.x; va[1] = v4.y; va[2] = v4.z; va[3] = v4.w;
+        } else {
+          const uint2 u = __ldg(reinterpret_cast<const uint2*>(vals + e0));
+          const float2 f0 = __half22float2(*reinterpret_cast<const __half2*>(&u.x));
+          const float2 f1 = __half22float2(*reinterpret_cast<const __half2*>(&u.y));
+          va[0] = f0.x; va[1] = f0.y; va[2] = f1.x; va[3] = f1.y;
+        }
+      } else {
 #pragma unroll
-      for (int i = 0; i < ITEMS; ++i) cc[i] = j0 + i < t_hi ? __ldg(cols + j0 + i) : 0;
-    }
-    if (vec_v && sizeof(VT) == 4) {
-#pragma unroll
-      for (int q = 0; q < ITEMS / 4; ++q) {
-        const float4 v4 = __ldg(reinterpret_cast<const float4*>(vals + j0) + q);
-        va[4 * q] = v4.x;
-        va[4 * q + 1] = v4.y;
-        va[4 * q + 2] = v4.z;
-        va[4 * q + 3] = v4.w;
-      }
-    } else if (vec_v) {
-#pragma unroll
-      for (int q = 0; q < ITEMS / 8; ++q) {
-        const uint4 u = __ldg(reinterpret_cast<const uint4*>(vals + j0) + q);
-        const __half2* h = reinterpret_cast<const __half2*>(&u);
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          const float2 f = __half22float2(h[k]);
-          va[8 * q + 2 * k] = f.x;
-          va[8 * q + 2 * k + 1] = f.y;
+        for (int i = 0; i < 4; ++i) {
+          const bool in = e0 + i < t_hi;
+          cc[i] = in ? __ldg(cols + e0 + i) : 0;
+          va[i] = in ? elem_f32<VT>(vals + e0 + i) : 0.f;
         }
       }
-    } else {
+      float pr[4];
 #pragma unroll
-      for (int i = 0; i < ITEMS; ++i) va[i] = j0 + i < t_hi ? elem_f32<VT>(vals + j0 + i) : 0.f;
+      for (int i = 0; i < 4; ++i) {
+        float xv = 0.f;
+        if ((unsigned long long)(unsigned)cc[i] < (unsigned long long)x_len) xv = elem_f32<VT>(x + cc[i]);
+        else if (e0 + i < t_hi && ws) record_error(ws, TCU_ERR_ARG, 301, (uint32_t)(e0 + i));
+        pr[i] = __fmul_rn(va[i], xv);
+      }
+      const int el = q * 128 + 4 * lane;  // element within the warp's 512
+      *reinterpret_cast<float4*>(&s_prod[w][el + (el >> 5) * 4]) = make_float4(pr[0], pr[1], pr[2], pr[3]);
     }
+    __syncwarp();
 #pragma unroll
-    for (int i = 0; i < ITEMS; ++i) {
-      float xv = 0.f;
-      if ((unsigned long long)(unsigned)cc[i] < (unsigned long long)x_len) xv = elem_f32<VT>(x + cc[i]);
-      else if (j0 + i < t_hi && ws) record_error(ws, TCU_ERR_ARG, 301, (uint32_t)(j0 + i));
-      p[i] = __fmul_rn(va[i], xv);
+    for (int c = 0; c < 4; ++c) {
+      const int el = 16 * lane + 4 * c;
+      const float4 f = *reinterpret_cast<const float4*>(&s_prod[w][el + (el >> 5) * 4]);
+      p[4 * c] = f.x; p[4 * c + 1] = f.y; p[4 * c + 2] = f.z; p[4 * c + 3] = f.w;
     }
   } else {
     if (vec_v) {

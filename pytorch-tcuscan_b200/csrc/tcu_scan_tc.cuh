@@ -115,11 +115,14 @@ struct ScanCfg {
   static constexpr int BPT = SMALL ? 1 : 256 / W;     // blocks per tile
   static constexpr int TILE_ELEMS = 128 * W * BPT;
   static constexpr int B_BYTES = W * RB;
-  static constexpr int OBW = W < 32 ? W : 32;         // output TMA box width (elements)
+  // columns staged per fill: the segmented modes stage whole rows (W); the
+  // full scans stage 64, or 32 at W = 64 and 16 for fp32 -- small enough
+  // that the staging area is double buffered next to the input stages, so
+  // a block's TMA store overlaps the next fill
+  static constexpr int FILLW = SEG ? W : (F16SPLIT ? 16 : (W == 64 ? 32 : (W < 64 ? W : 64)));
+  // output TMA box width (elements): at most 32 columns, within one fill
+  static constexpr int OBW = FILLW < 32 ? FILLW : 32;
   static constexpr int OSW = OBW * 4;                 // output box row bytes = swizzle span
-  // columns staged per fill: 64, or 32 for the fp32 full scan (a smaller
-  // staging area leaves room for a fifth input stage)
-  static constexpr int FILLW = (F16SPLIT && !SEG) ? 32 : (W < 64 ? W : 64);
   static constexpr int NFILL = W / FILLW;
   static constexpr int STG_BYTES = 128 * FILLW * 4;
   // Shared memory: input stage ring | U | output staging | control.  The ring
@@ -136,7 +139,7 @@ struct ScanCfg {
   static constexpr int RT_BYTES = F16SPLIT ? 2 * BPT * 128 * 8 : 0;
   static constexpr int FIXED = 1024 + CTRL_BYTES + B_ALLOC + MASK_BYTES + RS_BYTES + RT_BYTES;
   static constexpr int NST_DOUBLE = (kMaxSmem - FIXED - 4 * STG_BYTES) / STAGE_BYTES;
-  static constexpr int STG_BUFS = NST_DOUBLE >= 2 * BPT ? 2 : 1;
+  static constexpr int STG_BUFS = (NST_DOUBLE >= 2 * BPT || (F16SPLIT && !SEG && NST_DOUBLE > BPT)) ? 2 : 1;
   static constexpr int NST_FIT = (kMaxSmem - FIXED - 2 * STG_BUFS * STG_BYTES) / STAGE_BYTES;
   static constexpr int NST_CAP = 4 * BPT < 32 ? 4 * BPT : 32;
   static constexpr int NSTAGE = NST_FIT < NST_CAP ? NST_FIT : NST_CAP;
@@ -165,6 +168,7 @@ struct ScanCtrl {
   uint64_t drain;
   uint64_t agg_full[8];             // summer -> epilogue: tile aggregate published / bound index ready
   uint64_t agg_empty[8];            // epilogue -> summer: ring slot free
+  uint64_t rt_free[2];              // F16SPLIT: warpgroup g has read its row scales / totals (converters may refill)
   long long tile_i0[8];             // kSegBounds: first bound index >= tile start
   int wg_vote[2][4];
   uint32_t stage_cid[32];
@@ -485,6 +489,11 @@ __device__ __forceinline__ void scan_epilogue(const ScanParams& p, const CUtenso
     V rowex[BPT];
 #pragma unroll
     for (int j = 0; j < BPT; ++j) rowex[j] = V(0);
+    // F16SPLIT: the row scale factors of the tile, read here with the row
+    // totals so both arrays are free for the converters after phase A
+    float rsv[BPT];
+#pragma unroll
+    for (int j = 0; j < BPT; ++j) rsv[j] = C::F16SPLIT ? rsg[j * 128 + r] : 1.f;
     if constexpr (MODE != kScanRows) {
       uint32_t tb[BPT];
       if constexpr (!C::F16SPLIT) {
@@ -534,6 +543,7 @@ __device__ __forceinline__ void scan_epilogue(const ScanParams& p, const CUtenso
         }
       }
       named_bar_sync(bar_id, 128);
+      if (C::F16SPLIT && wg_thread == 0) mbar_arrive(&ctl->rt_free[g]);  // every thread has read rs / rt
       V run = V(0);
       int runf = 0;
 #pragma unroll
@@ -578,7 +588,6 @@ __device__ __forceinline__ void scan_epilogue(const ScanParams& p, const CUtenso
       int acci = 0;
       const float cf = IS_INT ? 0.f : (float)rowex[j];
       const uint32_t ci = IS_INT ? (uint32_t)(long long)rowex[j] : 0u;
-      const float rsv = C::F16SPLIT ? rsg[j * 128 + r] : 1.f;  // read before block j's slot is released
 #pragma unroll
       for (int h = 0; h < C::NFILL; ++h) {
         uint8_t* stg = stg_base + (nfill % C::STG_BUFS) * C::STG_BYTES;
@@ -593,7 +602,7 @@ __device__ __forceinline__ void scan_epilogue(const ScanParams& p, const CUtenso
         tmem_wait_ld();
         if constexpr (C::F16SPLIT) {  // undo the row's operand scale (a power of two: exact)
 #pragma unroll
-          for (int c = 0; c < C::FILLW; ++c) v[c] = __float_as_uint(__uint_as_float(v[c]) * rsv);
+          for (int c = 0; c < C::FILLW; ++c) v[c] = __float_as_uint(__uint_as_float(v[c]) * rsv[j]);
         }
         if (h == C::NFILL - 1) {
           tc_fence_before();
@@ -831,11 +840,11 @@ __device__ __forceinline__ void scan_summer(const ScanParams& p, uint8_t* smem, 
           if (SUMS) sum_split_rows(X0, C::TERM_BYTES, 0, 16, r_lo, vrows, acc);
           accd += (double)acc;
         } else {
-          // the row scales / totals of this TMEM half are free once the
-          // epilogue has drained block j of the tile two before this one
+          // the row scales / totals of this TMEM half are free once its
+          // warpgroup has read them for the tile two before this one
           const int g = i & 1;
           const uint32_t u = i >> 1;
-          if (u >= 1 && !__all_sync(0xffffffffu, mbar_wait(&ctl->slot_empty[g][j], (u & 1u) ^ 1u, wc, 11, i))) {
+          if (u >= 1 && !__all_sync(0xffffffffu, mbar_wait(&ctl->rt_free[g], (u - 1) & 1u, wc, 11, i))) {
             stop = true;
             break;
           }
@@ -1022,7 +1031,7 @@ __device__ __forceinline__ void scan_converter2(const ScanParams& p, uint8_t* sm
         } else {
           const int g = i & 1;
           const uint32_t u = i >> 1;
-          if (u >= 1 && !__all_sync(0xffffffffu, mbar_wait(&ctl->slot_empty[g][j], (u & 1u) ^ 1u, wc, 12, i))) {
+          if (u >= 1 && !__all_sync(0xffffffffu, mbar_wait(&ctl->rt_free[g], (u - 1) & 1u, wc, 12, i))) {
             if (lane == 0) mbar_arrive(&ctl->conv[s]);
             stop = true;
             break;
@@ -1182,6 +1191,11 @@ __device__ __forceinline__ void seg_epilogue(const ScanParams& p, const CUtensor
     // ---- (A) segmented row aggregates -> row offsets, tile aggregate ----
     V rowex[BPT];
     int exf[BPT];
+    // F16SPLIT: the row scale factors of the tile, read here with the row
+    // totals so both arrays are free for the converters after phase A
+    float rsv[BPT];
+#pragma unroll
+    for (int j = 0; j < BPT; ++j) rsv[j] = C::F16SPLIT ? rsg[j * 128 + r] : 1.f;
     {
       uint32_t tb[BPT];
       double tbd[BPT];  // F16SPLIT: row aggregates in FP64 (exact totals for rows without a start)
@@ -1208,9 +1222,8 @@ __device__ __forceinline__ void seg_epilogue(const ScanParams& p, const CUtensor
             tmem_ld16(tm + (uint32_t)(j * W + c * 16), *reinterpret_cast<uint32_t(*)[16]>(&v[c * 16]));
           tmem_wait_ld();
           if constexpr (C::F16SPLIT) {
-            const float rsv = rsg[j * 128 + r];
 #pragma unroll
-            for (int c = 0; c < W; ++c) v[c] = __float_as_uint(__uint_as_float(v[c]) * rsv);
+            for (int c = 0; c < W; ++c) v[c] = __float_as_uint(__uint_as_float(v[c]) * rsv[j]);
           }
           if (is_tail) {
             float accf = 0.f;
@@ -1277,6 +1290,7 @@ __device__ __forceinline__ void seg_epilogue(const ScanParams& p, const CUtensor
         }
       }
       named_bar_sync(bar_id, 128);
+      if (C::F16SPLIT && wg_thread == 0) mbar_arrive(&ctl->rt_free[g]);  // every thread has read rs / rt
       V run = V(0);
       int runf = 0;
 #pragma unroll
@@ -1324,7 +1338,6 @@ __device__ __forceinline__ void seg_epilogue(const ScanParams& p, const CUtensor
       int acci = 0;
       const float cf = IS_INT ? 0.f : (float)rowex[j];
       const uint32_t ci = IS_INT ? (uint32_t)(long long)rowex[j] : 0u;
-      const float rsv = C::F16SPLIT ? rsg[j * 128 + r] : 1.f;  // read before block j's slot is released
       uint8_t* stg = stg_base + (nfill % C::STG_BUFS) * C::STG_BYTES;
       // per-segment sums: the first chunk of this block's bounds is loaded
       // now, its latency hidden behind the row work below
@@ -1348,7 +1361,7 @@ __device__ __forceinline__ void seg_epilogue(const ScanParams& p, const CUtensor
       if (lane == 0) mbar_arrive(&ctl->slot_empty[g][j]);
       if constexpr (C::F16SPLIT) {  // undo the row's operand scale (a power of two: exact)
 #pragma unroll
-        for (int c = 0; c < W; ++c) v[c] = __float_as_uint(__uint_as_float(v[c]) * rsv);
+        for (int c = 0; c < W; ++c) v[c] = __float_as_uint(__uint_as_float(v[c]) * rsv[j]);
       }
       if (is_tail) {
 #pragma unroll
@@ -1483,6 +1496,8 @@ __global__ void __launch_bounds__(kThreads, 1)
       mbar_init(&ctl->agg_full[m], 1);
       mbar_init(&ctl->agg_empty[m], 1);
     }
+    mbar_init(&ctl->rt_free[0], 1);
+    mbar_init(&ctl->rt_free[1], 1);
     for (int g = 0; g < 2; ++g) {
       mbar_init(&ctl->tile_full[g], 2);  // tcgen05.commit + releasing arrive after tile_cid
       for (int j = 0; j < BPT; ++j) mbar_init(&ctl->slot_empty[g][j], 4);  // one arrive per epilogue warp
