@@ -234,6 +234,35 @@ def measure_extras(dev, steps=10, warmup=3):
     out["topk_f16_20Mi_ksqrt"] = entry(nt, nt * 2, ms, k=kt)
     del xt
 
+    # block scan (every S*S tile scanned), fp16, 2^26 elements, S = 128: the
+    # reference's tensor-only formulation (three products per 128-row block,
+    # tcu_block_scan_tensor, run_block_scan's path) against the scan engine's
+    # block mode (one product, exact shuffle row offsets, tcu_block_scan)
+    from tcuscan_ops import _lib as L
+
+    nb = 1 << 26
+    xb = workloads.scan_input(nb, torch.float16, dev, seed=14)
+    ones = torch.ones(128, 128, dtype=torch.float16, device=dev)
+    up, lo = torch.triu(ones), torch.tril(ones, -1)
+    ms_t = _device_ms(lambda: tcuscan_ops.run_block_scan(xb, up, lo), steps, warmup)
+    zt = tcuscan_ops.run_block_scan(xb, up, lo)
+    zb = torch.empty(nb, dtype=torch.float32, device=dev)
+    ws, wsb, sp = L.launch_context(dev, L.lib.tcu_workspace_bytes(nb, 128))
+
+    def engine_block():
+        tcuscan_ops.check(L.lib.tcu_block_scan(xb.data_ptr(), L.TCU_FLOAT16, nb, 128, zb.data_ptr(), ws, wsb, sp),
+                          "tcu_block_scan")
+    ms_e = _device_ms(engine_block, steps, warmup)
+    engine_block()
+    refb = torch.cumsum(xb.double().reshape(-1, 128 * 128), 1).reshape(-1)
+    err_t = ((zt.double() - refb).abs() / refb.abs().clamp_min(1.0)).max().item()
+    err_e = ((zb.double() - refb).abs() / refb.abs().clamp_min(1.0)).max().item()
+    out["block_scan_f16_2e26_tensor_only"] = entry(nb, 6 * nb, ms_t, S=128, max_rel_err_vs_fp64=err_t,
+                                                   kernel="block_scan_tc_kernel (A.U + L.(A.J))")
+    out["block_scan_f16_2e26_engine"] = entry(nb, 6 * nb, ms_e, S=128, max_rel_err_vs_fp64=err_e,
+                                              kernel="scan_tc_kernel kScanBlocks (A.U, shuffle offsets)")
+    del xb, zt, zb, refb
+
     # flag-driven segmented scan (starts), fp16 2^28, flags Bernoulli(0.01)
     xf = workloads.scan_input(n, torch.float16, dev, seed=12)
     fl = workloads.bernoulli_mask(n, 0.01, dev, seed=13)
@@ -517,7 +546,7 @@ def _sig(v, digits=4):
 
 
 LEG_KEYS = ("scan_f16_2e28", "compress_f16", "compress_f32", "seg_scan_flags_f16_2e28", "spmv_f32", "spmv_f16",
-            "batch_rows_f32_4096", "scan_f16_2e20")
+            "batch_rows_f32_4096", "scan_f16_2e20", "block_scan_f16_2e26_tensor_only", "block_scan_f16_2e26_engine")
 
 
 def legs_summary(extras):

@@ -183,6 +183,19 @@ TCU_API tcu_status_t tcu_row_scan(const void* x, tcu_dtype_t x_dtype, int64_t n_
 TCU_API tcu_status_t tcu_block_scan(const void* x, tcu_dtype_t x_dtype, int64_t n, int S, void* z, void* ws,
                             size_t ws_bytes, void* stream);
 
+/* Block scan in the reference's tensor-only formulation: for every S x S
+ * tile A of fp16 x (S = 64 or 128; n a multiple of S*S) z = A.upper +
+ * lower_strict.(A.J) with J all ones, every product on the tensor cores
+ * (the row totals A.J go back in as a three-term fp16 operand on a per-block
+ * power-of-two scale, FP32 accumulation).  upper / lower_strict: the
+ * caller's S x S fp16 row-major matrices on the device, used as given.
+ * ws: a workspace (device-side wait errors are recorded there).  Replaces
+ * run_block_scan (src/torch/torch_scan.h:362-405) with the reference's
+ * multi-cube kernel (src/kernels/kernel_block_scan.h:23-40).              */
+TCU_API tcu_status_t tcu_block_scan_tensor(const void* x, tcu_dtype_t x_dtype, int64_t n, int S, const void* upper,
+                                           const void* lower_strict, void* z, void* ws, size_t ws_bytes,
+                                           void* stream);
+
 /* ---- segmented scans (tensor cores) ---------------------------------------
  * Segmented inclusive scan of x (int8 -> int32 exact, fp16 -> fp32, fp32 ->
  * fp32 via split-precision bf16 hi + lo operands).

@@ -115,11 +115,10 @@ struct ScanCfg {
   static constexpr int BPT = SMALL ? 1 : 256 / W;     // blocks per tile
   static constexpr int TILE_ELEMS = 128 * W * BPT;
   static constexpr int B_BYTES = W * RB;
-  // columns staged per fill: the segmented modes stage whole rows (W); the
-  // full scans stage 64, or 32 at W = 64 and 16 for fp32 -- small enough
-  // that the staging area is double buffered next to the input stages, so
-  // a block's TMA store overlaps the next fill
-  static constexpr int FILLW = SEG ? W : (F16SPLIT ? 16 : (W == 64 ? 32 : (W < 64 ? W : 64)));
+  // columns staged per fill: whole rows up to 64 columns.  Narrower,
+  // double-buffered fills (32 columns at W = 64, 16 for fp32) were measured
+  // slower for fp16 and fp32 alike: each fill costs two warpgroup barriers.
+  static constexpr int FILLW = W < 64 ? W : 64;
   // output TMA box width (elements): at most 32 columns, within one fill
   static constexpr int OBW = FILLW < 32 ? FILLW : 32;
   static constexpr int OSW = OBW * 4;                 // output box row bytes = swizzle span
@@ -139,7 +138,7 @@ struct ScanCfg {
   static constexpr int RT_BYTES = F16SPLIT ? 2 * BPT * 128 * 8 : 0;
   static constexpr int FIXED = 1024 + CTRL_BYTES + B_ALLOC + MASK_BYTES + RS_BYTES + RT_BYTES;
   static constexpr int NST_DOUBLE = (kMaxSmem - FIXED - 4 * STG_BYTES) / STAGE_BYTES;
-  static constexpr int STG_BUFS = (NST_DOUBLE >= 2 * BPT || (F16SPLIT && !SEG && NST_DOUBLE > BPT)) ? 2 : 1;
+  static constexpr int STG_BUFS = NST_DOUBLE >= 2 * BPT ? 2 : 1;
   static constexpr int NST_FIT = (kMaxSmem - FIXED - 2 * STG_BUFS * STG_BYTES) / STAGE_BYTES;
   static constexpr int NST_CAP = 4 * BPT < 32 ? 4 * BPT : 32;
   static constexpr int NSTAGE = NST_FIT < NST_CAP ? NST_FIT : NST_CAP;

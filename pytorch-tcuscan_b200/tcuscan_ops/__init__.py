@@ -143,7 +143,13 @@ def run_row_scan(x, S):
 
 def run_block_scan(x, upper, lower_strict):
     """Scan of every consecutive S*S block; n % S*S == 0 (reference:
-    src/torch/torch_scan.h:362-405, kernel_block_scan.h:62-67)."""
+    src/torch/torch_scan.h:362-405, kernel_block_scan.h:62-67).
+
+    float16 at S = 64 / 128 runs the reference's tensor-only formulation
+    (tcu_block_scan_tensor: z = A.upper + lower_strict.(A.J) per tile, every
+    product on the tensor cores, the caller's matrices used as given);
+    other S and int8 run the scan engine's block mode, which builds the
+    standard triangular operand on chip and reads only the matrices' shape."""
     S = _check_tri(upper, lower_strict)
     x = _cuda_input(x)
     n = x.numel()
@@ -151,6 +157,15 @@ def run_block_scan(x, upper, lower_strict):
         raise ValueError(f"run_block_scan: numel {n} must be a multiple of S*S={S * S}")
     z = torch.empty(n, dtype=_scan_out_dtype(x.dtype), device=x.device)
     if n == 0:
+        return z
+    if x.dtype == torch.float16 and S in (64, 128):
+        up = _cuda_input(upper.to(device=x.device, dtype=torch.float16), "upper")
+        lo = _cuda_input(lower_strict.to(device=x.device, dtype=torch.float16), "lower_strict")
+        ws, wsb, sp = _lib.launch_context(x.device, 256)
+        st = _lib.lib.tcu_block_scan_tensor(x.data_ptr(), _lib.TCU_FLOAT16, n, S, up.data_ptr(), lo.data_ptr(),
+                                            z.data_ptr(), ws, wsb, sp)
+        check(st, "run_block_scan")
+        _after(x)
         return z
     ws, wsb = workspace(x.device, _lib.lib.tcu_workspace_bytes(n, S))
     st = _lib.lib.tcu_block_scan(x.data_ptr(), _lib.DTYPE_CODE[x.dtype], n, S, z.data_ptr(), ws, wsb,

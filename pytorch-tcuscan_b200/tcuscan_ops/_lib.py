@@ -76,6 +76,7 @@ _sig("tcu_scan_chained_typed", _ST, _P, _I, _I64, _I, _D, _P, _I, _P, _P, _SZ, _
 _sig("tcu_total", _ST, _P, _I, _I64, _P, _P, _SZ, _P)
 _sig("tcu_row_scan", _ST, _P, _I, _I64, _I, _P, _P, _SZ, _P)
 _sig("tcu_block_scan", _ST, _P, _I, _I64, _I, _P, _P, _SZ, _P)
+_sig("tcu_block_scan_tensor", _ST, _P, _I, _I64, _I, _P, _P, _P, _P, _SZ, _P)
 _sig("tcu_seg_scan", _ST, _P, _I, _I64, _I, _P, _I, _P, _P, _SZ, _P)
 _sig("tcu_seg_bounds", _ST, _P, _I, _I64, _I, _P, _I, _I64, _I, _P, _P, _SZ, _P)
 _sig("tcu_scan_batch", _ST, _P, _I, _I64, _I64, _I, _P, _P, _SZ, _P)
