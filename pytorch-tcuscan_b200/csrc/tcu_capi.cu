@@ -221,7 +221,7 @@ static tcu_status_t launch_scan_tc(const void* x, int64_t n, void* z, double sta
   }
   int grid = grid_ctas();
   if (p.num_tiles < grid) grid = (int)p.num_tiles;
-  kern<<<grid, kThreads, smem, st>>>(in_map, out_map, p);
+  kern<<<grid, C::THREADS, smem, st>>>(in_map, out_map, p);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "scan_tc_kernel launch");
   if (tile_first) {

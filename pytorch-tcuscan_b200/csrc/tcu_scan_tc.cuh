@@ -90,7 +90,7 @@ __device__ __forceinline__ void phase_add(const ScanParams& p, int k, uint64_t d
 }
 
 constexpr uint32_t kSentinel = 0xFFFFFFFFu;
-constexpr int kThreads = 384;  // 12 warps: producer, MMA, 2 epilogue warpgroups, summer, second fp32 converter
+constexpr int kThreads = 384;  // 12 warps: producer, MMA, 2 epilogue warpgroups, summer, second summer / converter
 constexpr int kMaxSmem = 232448;
 
 template <typename InT, int W, bool SEG = false, bool SMALL = false>
@@ -128,7 +128,7 @@ struct ScanCfg {
   // holds as many blocks as fit (at least one tile, at most four); output
   // staging is double buffered unless that would leave under two tiles of
   // input stages.
-  static constexpr int CTRL_BYTES = 3328;
+  static constexpr int CTRL_BYTES = 3840;
   static constexpr int B_ALLOC = ((B_BYTES + 1023) / 1024) * 1024;
   // segmented modes keep one 64-bit start mask per row of a tile per warpgroup
   static constexpr int MASK_BYTES = SEG ? 2 * BPT * 128 * 8 : 0;
@@ -137,6 +137,11 @@ struct ScanCfg {
   static constexpr int RS_BYTES = F16SPLIT ? 2 * BPT * 128 * 4 : 0;
   static constexpr int RT_BYTES = F16SPLIT ? 2 * BPT * 128 * 8 : 0;
   static constexpr int FIXED = 1024 + CTRL_BYTES + B_ALLOC + MASK_BYTES + RS_BYTES + RT_BYTES;
+  // threads per CTA: 12 warps, or 14 for the fp32 split (four converter
+  // warps, warps 10-13, 32 rows of every stage each: the conversion is the
+  // most instruction-heavy stage of the pipeline)
+  static constexpr int THREADS = F16SPLIT ? 448 : kThreads;
+  static constexpr int NCONV = F16SPLIT ? 4 : 2;  // warps arriving on conv[s] (fp32 converters / fp16 summers)
   static constexpr int NST_DOUBLE = (kMaxSmem - FIXED - 4 * STG_BYTES) / STAGE_BYTES;
   static constexpr int STG_BUFS = NST_DOUBLE >= 2 * BPT ? 2 : 1;
   static constexpr int NST_FIT = (kMaxSmem - FIXED - 2 * STG_BUFS * STG_BYTES) / STAGE_BYTES;
@@ -161,7 +166,7 @@ struct ScanCtrl {
   uint64_t full[32];
   uint64_t empty[32];
   uint64_t conv[32];                // fp32: stage converted to bf16 hi/lo operands (two converter warps)
-  double cv_sum[32];                // fp32: sum of a stage's rows 64-127 (second converter)
+  double cv_sum[32][3];             // partial stage sums of the converters / second summer after warp 10
   uint64_t tile_full[2];
   uint64_t slot_empty[2][16];
   uint64_t drain;
@@ -180,7 +185,7 @@ struct ScanCtrl {
   uint8_t wt_flag[2][16][4];        // warp segment flags per block
   LbScratch lb[2];
 };
-static_assert(sizeof(ScanCtrl) <= 3328, "control block");
+static_assert(sizeof(ScanCtrl) <= 3840, "control block");
 
 // Value of 1 in the MMA operand encoding.
 template <typename T>
@@ -236,6 +241,30 @@ __device__ __forceinline__ void seg_combine(int& f, V& v, int f_prev, V v_prev) 
   f |= f_prev;
 }
 
+// Pairs of fp32 values in one 64-bit register pair (Blackwell f32x2
+// arithmetic: both lanes rounded to nearest, as the scalar instructions).
+typedef unsigned long long f32x2_t;
+__device__ __forceinline__ f32x2_t f2_make(float a, float b) {
+  return (f32x2_t)__float_as_uint(a) | ((f32x2_t)__float_as_uint(b) << 32);
+}
+__device__ __forceinline__ float f2_lo(f32x2_t p) { return __uint_as_float((uint32_t)p); }
+__device__ __forceinline__ float f2_hi(f32x2_t p) { return __uint_as_float((uint32_t)(p >> 32)); }
+__device__ __forceinline__ f32x2_t f2_add(f32x2_t a, f32x2_t b) {
+  f32x2_t d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ f32x2_t f2_sub(f32x2_t a, f32x2_t b) {
+  f32x2_t d;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ f32x2_t f2_mul(f32x2_t a, f32x2_t b) {
+  f32x2_t d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+
 // In-place split of rows [row0, row1) of an fp32 block into the two fp16
 // MMA operand tiles, with every row's exact total; one lane per row (32 rows
 // per pass, no cross-lane work).  Each 64-column row arrives as two 128-byte
@@ -260,43 +289,44 @@ __device__ __forceinline__ void convert_f32_rows(uint8_t* X0, int term_bytes, in
   uint8_t* X1 = X0 + term_bytes;
   const int lane = threadIdx.x & 31;
   const float kRound16 = 201326592.0f;  // 1.5 * 2^27: (y + c) - c rounds y to a multiple of 16
+  const f32x2_t c2 = f2_make(kRound16, kRound16);
 #pragma unroll 1
   for (int row = row0 + lane; row < row1; row += 32) {
-    float v[64];
+    f32x2_t v[32];  // the row's 64 values as pairs (columns 2i, 2i + 1)
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
       const uint32_t off = swz(row * 128 + c * 16, 128);
-      const float4 a = *reinterpret_cast<const float4*>(X0 + off);
-      const float4 b = *reinterpret_cast<const float4*>(X1 + off);
-      v[4 * c] = a.x; v[4 * c + 1] = a.y; v[4 * c + 2] = a.z; v[4 * c + 3] = a.w;
-      v[32 + 4 * c] = b.x; v[33 + 4 * c] = b.y; v[34 + 4 * c] = b.z; v[35 + 4 * c] = b.w;
+      const ulonglong2 a = *reinterpret_cast<const ulonglong2*>(X0 + off);
+      const ulonglong2 b = *reinterpret_cast<const ulonglong2*>(X1 + off);
+      v[2 * c] = a.x; v[2 * c + 1] = a.y;
+      v[16 + 2 * c] = b.x; v[17 + 2 * c] = b.y;
     }
     float mx[8];
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      mx[q] = fmaxf(fmaxf(fabsf(v[8 * q]), fabsf(v[8 * q + 1])), fmaxf(fabsf(v[8 * q + 2]), fabsf(v[8 * q + 3])));
-      mx[q] = fmaxf(mx[q], fmaxf(fmaxf(fabsf(v[8 * q + 4]), fabsf(v[8 * q + 5])),
-                                 fmaxf(fabsf(v[8 * q + 6]), fabsf(v[8 * q + 7]))));
-    }
+    for (int q = 0; q < 8; ++q)
+      mx[q] = fmaxf(fmaxf(fmaxf(fabsf(f2_lo(v[4 * q])), fabsf(f2_hi(v[4 * q]))),
+                          fmaxf(fabsf(f2_lo(v[4 * q + 1])), fabsf(f2_hi(v[4 * q + 1])))),
+                    fmaxf(fmaxf(fabsf(f2_lo(v[4 * q + 2])), fabsf(f2_hi(v[4 * q + 2]))),
+                          fmaxf(fabsf(f2_lo(v[4 * q + 3])), fabsf(f2_hi(v[4 * q + 3])))));
     const float m = fmaxf(fmaxf(fmaxf(mx[0], mx[1]), fmaxf(mx[2], mx[3])),
                           fmaxf(fmaxf(mx[4], mx[5]), fmaxf(mx[6], mx[7])));
     const int eb = (int)((__float_as_uint(m) >> 23) & 0xFFu);  // biased exponent of the row's max
     int k = eb == 0xFF ? 0 : 141 - eb;                          // 14 - (eb - 127)
     k = k > 126 ? 126 : k;                                      // k >= -113 always
     const float sc = __uint_as_float((uint32_t)(k + 127) << 23);
-    float shi[4] = {0.f, 0.f, 0.f, 0.f}, sr[4] = {0.f, 0.f, 0.f, 0.f};
+    const f32x2_t sc2 = f2_make(sc, sc);
+    f32x2_t shi[2] = {0ull, 0ull}, sr[2] = {0ull, 0ull};
 #pragma unroll
     for (int c = 0; c < 8; ++c) {  // output chunk c: columns 8c .. 8c + 7 of the hi and lo rows
       uint32_t hw[4], lw[4];
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
-        const float y0 = v[8 * c + 2 * e] * sc, y1 = v[8 * c + 2 * e + 1] * sc;
-        const float h0 = __fadd_rn(__fadd_rn(y0, kRound16), -kRound16);
-        const float h1 = __fadd_rn(__fadd_rn(y1, kRound16), -kRound16);
-        const float r0 = __fadd_rn(y0, -h0), r1 = __fadd_rn(y1, -h1);
-        shi[e] = __fadd_rn(shi[e], __fadd_rn(h0, h1));
-        sr[e] = __fadd_rn(sr[e], __fadd_rn(r0, r1));
-        const __half2 hh = __floats2half2_rn(h0, h1), ll = __floats2half2_rn(r0, r1);
+        const f32x2_t y = f2_mul(v[4 * c + e], sc2);
+        const f32x2_t h = f2_sub(f2_add(y, c2), c2);
+        const f32x2_t r = f2_sub(y, h);
+        shi[e & 1] = f2_add(shi[e & 1], h);
+        sr[e & 1] = f2_add(sr[e & 1], r);
+        const __half2 hh = __floats2half2_rn(f2_lo(h), f2_hi(h)), ll = __floats2half2_rn(f2_lo(r), f2_hi(r));
         hw[e] = *reinterpret_cast<const uint32_t*>(&hh);
         lw[e] = *reinterpret_cast<const uint32_t*>(&ll);
       }
@@ -304,8 +334,9 @@ __device__ __forceinline__ void convert_f32_rows(uint8_t* X0, int term_bytes, in
       *reinterpret_cast<uint4*>(X0 + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
       *reinterpret_cast<uint4*>(X1 + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
     }
-    const float th = __fadd_rn(__fadd_rn(shi[0], shi[1]), __fadd_rn(shi[2], shi[3]));  // exact
-    const float tr = __fadd_rn(__fadd_rn(sr[0], sr[1]), __fadd_rn(sr[2], sr[3]));
+    const f32x2_t sh = f2_add(shi[0], shi[1]), sl = f2_add(sr[0], sr[1]);
+    const float th = __fadd_rn(f2_lo(sh), f2_hi(sh));  // exact
+    const float tr = __fadd_rn(f2_lo(sl), f2_hi(sl));
     const float rsc = __uint_as_float((uint32_t)(127 - k) << 23);  // 2^-k
     const double tot = ((double)th + (double)tr) * (double)rsc;
     rs_out[row] = rsc;
@@ -397,7 +428,7 @@ __device__ __forceinline__ void build_upper(uint8_t* bmat) {
   using C = ScanCfg<InT, W>;
   constexpr int CPR = C::RB / 16;  // 16-byte chunks per row
   const uint32_t one = one_bits<typename OperandT<InT>::T>();
-  for (int t = threadIdx.x; t < W * CPR; t += kThreads) {
+  for (int t = threadIdx.x; t < W * CPR; t += blockDim.x) {
     const int nrow = t / CPR, c = t % CPR;
     const int kb = (c * 16) / C::SW, cin = c % (C::SW / 16);
     const int k0 = (kb * C::SW + cin * 16) / C::ELEM;
@@ -848,15 +879,16 @@ __device__ __forceinline__ void scan_summer(const ScanParams& p, uint8_t* smem, 
             break;
           }
           const int rix = (g * BPT + j) * 128;
-          convert_f32_rows(X0, C::TERM_BYTES, 0, 64, r_lo, vrows, SUMS, accd,
+          convert_f32_rows(X0, C::TERM_BYTES, 0, 128 / C::NCONV, r_lo, vrows, SUMS, accd,
                            reinterpret_cast<float*>(smem + C::OFF_RS) + rix,
                            reinterpret_cast<double*>(smem + C::OFF_RT) + rix);
         }
         if (lane == 0) mbar_arrive(&ctl->conv[s]);
-        if constexpr (SUMS) {  // the other half's sum, stored before its conv arrival
+        if constexpr (SUMS) {  // the other converters' sums, stored before their conv arrivals
           const bool okc = __all_sync(0xffffffffu, mbar_wait(&ctl->conv[s], (k / C::NSTAGE) & 1u, wc, 9, i));
           if (!okc) { stop = true; break; }
-          if (lane == 0) accd += ctl->cv_sum[s];
+          if (lane == 0)
+            for (int c = 0; c < C::NCONV - 1; ++c) accd += ctl->cv_sum[s][c];
         }
       }
       if constexpr (SUMS && !C::IS_F32) {
@@ -877,7 +909,7 @@ __device__ __forceinline__ void scan_summer(const ScanParams& p, uint8_t* smem, 
           if (lane == 0) mbar_arrive(&ctl->conv[s]);
           const bool okc = __all_sync(0xffffffffu, mbar_wait(&ctl->conv[s], (k / C::NSTAGE) & 1u, wc, 13, i));
           if (!okc) { stop = true; break; }
-          if (lane == 0) accd += ctl->cv_sum[s];
+          if (lane == 0) accd += ctl->cv_sum[s][0];
         }
       }
       __syncwarp();
@@ -956,7 +988,7 @@ __device__ __forceinline__ void scan_summer(const ScanParams& p, uint8_t* smem, 
 // publishes) in cv_sum[s] before its conv arrival.  Idle otherwise.
 template <typename InT, int W, int MODE>
 __device__ __forceinline__ void scan_converter2(const ScanParams& p, uint8_t* smem, ScanCtrl* ctl,
-                                                const WaitCtx& wc) {
+                                                const WaitCtx& wc, int cidx) {
   using C = ScanCfg<InT, W, is_seg(MODE), MODE == kScanFullSmall>;
   constexpr bool SUMS_ANY = (is_full(MODE) || MODE == kSegBounds || MODE == kSegPeriodic);
   if constexpr (!C::IS_F32 && !C::IS_INT && SUMS_ANY) {
@@ -987,7 +1019,7 @@ __device__ __forceinline__ void scan_converter2(const ScanParams& p, uint8_t* sm
         float accf = 0.f;
         sum_stage_rows<InT, W>(smem + s * C::STAGE_BYTES, r_lo > 64 ? r_lo : 64, vrows, acci, accf);
         const double t = warp_sum_any((double)accf);
-        if (lane == 0) ctl->cv_sum[s] = t;
+        if (lane == 0) ctl->cv_sum[s][0] = t;
         __syncwarp();
         if (lane == 0) mbar_arrive(&ctl->conv[s]);
       }
@@ -1036,13 +1068,14 @@ __device__ __forceinline__ void scan_converter2(const ScanParams& p, uint8_t* sm
             break;
           }
           const int rix = (g * BPT + j) * 128;
-          convert_f32_rows(smem + s * C::STAGE_BYTES, C::TERM_BYTES, 64, 128, r_lo, vrows, SUMS, acc,
+          constexpr int RPC = 128 / C::NCONV;  // rows per converter
+          convert_f32_rows(smem + s * C::STAGE_BYTES, C::TERM_BYTES, cidx * RPC, (cidx + 1) * RPC, r_lo, vrows, SUMS, acc,
                            reinterpret_cast<float*>(smem + C::OFF_RS) + rix,
                            reinterpret_cast<double*>(smem + C::OFF_RT) + rix);
         }
         if constexpr (SUMS) {
           const double t = warp_sum_any(acc);
-          if (lane == 0) ctl->cv_sum[s] = t;
+          if (lane == 0) ctl->cv_sum[s][cidx - 1] = t;
         }
         __syncwarp();
         if (lane == 0) mbar_arrive(&ctl->conv[s]);
@@ -1468,7 +1501,7 @@ __device__ __forceinline__ void seg_epilogue(const ScanParams& p, const CUtensor
 }
 
 template <typename InT, int W, int MODE>
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(ScanCfg<InT, W, is_seg(MODE), MODE == kScanFullSmall>::THREADS, 1)
     scan_tc_kernel(const __grid_constant__ CUtensorMap in_map, const __grid_constant__ CUtensorMap out_map,
                    const ScanParams p) {
   using C = ScanCfg<InT, W, is_seg(MODE), MODE == kScanFullSmall>;
@@ -1489,7 +1522,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     for (int s = 0; s < C::NSTAGE; ++s) {
       mbar_init(&ctl->full[s], 1);
       mbar_init(&ctl->empty[s], 2);  // MMA commit + summer/converter arrive
-      mbar_init(&ctl->conv[s], 2);
+      mbar_init(&ctl->conv[s], C::NCONV);
     }
     for (int m = 0; m < 8; ++m) {
       mbar_init(&ctl->agg_full[m], 1);
@@ -1527,7 +1560,11 @@ __global__ void __launch_bounds__(kThreads, 1)
     // A tile id is taken only once every stage of that tile is free, and all
     // of its blocks are then issued at once: the time from taking an id to
     // its aggregate being published is one TMA round trip, never this CTA's
-    // backlog.
+    // backlog.  fp32 launches, whose ring holds one tile (4 stages of 32 KB),
+    // take the id when the tile's first stage is free and issue each later
+    // block as its stage frees, so the next tile's loads overlap the current
+    // tile's conversion instead of following it.
+    constexpr int kWaitFirst = (C::F16SPLIT && C::NSTAGE < 2 * BPT) ? 1 : BPT;
     if (lane == 0) {
       uint32_t issued[32];
 #pragma unroll
@@ -1536,7 +1573,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       bool stop = false;
       while (!stop) {
         const uint64_t tw = p.phase_ns ? globaltimer() : 0;
-        for (int j = 0; j < BPT && !stop; ++j) {
+        for (int j = 0; j < kWaitFirst && !stop; ++j) {
           const uint32_t kj = k + j;
           const int s = kj % C::NSTAGE;
           if (kj >= (uint32_t)C::NSTAGE && !mbar_wait(&ctl->empty[s], ((kj / C::NSTAGE) & 1u) ^ 1u, wc, 1, kj))
@@ -1549,6 +1586,11 @@ __global__ void __launch_bounds__(kThreads, 1)
         const int nblk = live ? BPT : 1;
         for (int j = 0; j < nblk; ++j, ++k) {
           const int s = k % C::NSTAGE;
+          if (j >= kWaitFirst && k >= (uint32_t)C::NSTAGE &&
+              !mbar_wait(&ctl->empty[s], ((k / C::NSTAGE) & 1u) ^ 1u, wc, 1, k)) {
+            stop = true;
+            break;
+          }
           ctl->stage_cid[s] = live ? tid : kSentinel;
           issued[s]++;
           const int64_t row0 = ((int64_t)tid * BPT + j) * 128;
@@ -1643,7 +1685,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   } else if (warp == 10) {
     scan_summer<InT, W, MODE>(p, smem, ctl, epoch, wc);
   } else {
-    scan_converter2<InT, W, MODE>(p, smem, ctl, wc);
+    scan_converter2<InT, W, MODE>(p, smem, ctl, wc, warp - 10);
   }
 
   // ---- teardown ----
