@@ -687,7 +687,7 @@ def run_reference_arm(args):
 
 
 PROFILE_OPS = ("compress_f16", "compress_f32", "compress_ind_f16", "spmv_f32", "spmv_f16", "serve", "segscan_i8",
-               "segscan_f16", "segsum_i8", "segsum_f16", "segsum_f32", "split_f16", "sort_f16", "topk_f16",
+               "segscan_f16", "segscan_f32", "segsum_i8", "segsum_f16", "segsum_f32", "split_f16", "sort_f16", "topk_f16",
                "rowsum_f16", "scan_i8", "scan_f16", "scan_f32", "segflags_f16")
 
 

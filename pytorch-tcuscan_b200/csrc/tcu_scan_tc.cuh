@@ -264,6 +264,14 @@ __device__ __forceinline__ f32x2_t f2_mul(f32x2_t a, f32x2_t b) {
   asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
   return d;
 }
+__device__ __forceinline__ f32x2_t f2_fma(f32x2_t a, f32x2_t b, f32x2_t c) {
+  f32x2_t d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+__device__ __forceinline__ f32x2_t f2_bits(uint32_t a, uint32_t b) {
+  return (f32x2_t)a | ((f32x2_t)b << 32);
+}
 
 // In-place split of rows [row0, row1) of an fp32 block into the two fp16
 // MMA operand tiles, with every row's exact total; one lane per row (32 rows
@@ -630,33 +638,56 @@ __device__ __forceinline__ void scan_epilogue(const ScanParams& p, const CUtenso
         for (int c = 0; c < C::FILLW / 16; ++c)
           tmem_ld16(tm + (uint32_t)(j * W + h * C::FILLW + c * 16), *reinterpret_cast<uint32_t(*)[16]>(&v[c * 16]));
         tmem_wait_ld();
-        if constexpr (C::F16SPLIT) {  // undo the row's operand scale (a power of two: exact)
-#pragma unroll
-          for (int c = 0; c < C::FILLW; ++c) v[c] = __float_as_uint(__uint_as_float(v[c]) * rsv[j]);
-        }
         if (h == C::NFILL - 1) {
           tc_fence_before();
           __syncwarp();
           if (lane == 0) mbar_arrive(&ctl->slot_empty[g][j]);  // block j's TMEM columns are free
         }
-        if (is_tail) {
+        if (!is_tail) {
+          // y = z + carry (fp32 split: z * 2^-k + carry, the scale a power of
+          // two so the product is exact and the fused form rounds once, as
+          // the separate multiply and add do), two columns per instruction
+#pragma unroll
+          for (int e4 = 0; e4 < C::FILLW / 4; ++e4) {
+            uint4 o;
+            const uint32_t* ve = &v[e4 * 4];
+            if constexpr (IS_INT) {
+              o = make_uint4(ve[0] + ci, ve[1] + ci, ve[2] + ci, ve[3] + ci);
+            } else {
+              const f32x2_t c2 = f2_make(cf, cf);
+              f32x2_t a = f2_bits(ve[0], ve[1]), b = f2_bits(ve[2], ve[3]);
+              if constexpr (C::F16SPLIT) {
+                const f32x2_t s2 = f2_make(rsv[j], rsv[j]);
+                a = f2_fma(a, s2, c2);
+                b = f2_fma(b, s2, c2);
+              } else {
+                a = f2_add(a, c2);
+                b = f2_add(b, c2);
+              }
+              o = make_uint4((uint32_t)a, (uint32_t)(a >> 32), (uint32_t)b, (uint32_t)(b >> 32));
+            }
+            const int cc = e4 * 4;
+            const int box = cc / C::OBW, cin = cc % C::OBW;
+            *(uint4*)(stg + box * (128 * C::OSW) + swz(r * C::OSW + cin * 4, C::OSW)) = o;
+          }
+        } else {
+          // the ragged last row: prefixes from global memory, written to z
+          // directly as well as staged
 #pragma unroll
           for (int c = 0; c < C::FILLW / 16; ++c)
             tail_chunk<InT, W>(p, h * C::FILLW + c * 16, *reinterpret_cast<uint32_t(*)[16]>(&v[c * 16]), accf, acci);
-        }
 #pragma unroll
-        for (int e4 = 0; e4 < C::FILLW / 4; ++e4) {
-          uint32_t o[4];
+          for (int e4 = 0; e4 < C::FILLW / 4; ++e4) {
+            uint32_t o[4];
 #pragma unroll
-          for (int e = 0; e < 4; ++e) {
-            if constexpr (IS_INT) o[e] = v[e4 * 4 + e] + ci;
-            else o[e] = __float_as_uint(__uint_as_float(v[e4 * 4 + e]) + cf);
-          }
-          const int cc = e4 * 4;
-          const int box = cc / C::OBW, cin = cc % C::OBW;
-          uint8_t* dst = stg + box * (128 * C::OSW) + swz(r * C::OSW + cin * 4, C::OSW);
-          *(uint4*)dst = make_uint4(o[0], o[1], o[2], o[3]);
-          if (is_tail) {
+            for (int e = 0; e < 4; ++e) {
+              if constexpr (IS_INT) o[e] = v[e4 * 4 + e] + ci;
+              else o[e] = __float_as_uint(__uint_as_float(v[e4 * 4 + e]) + cf);
+            }
+            const int cc = e4 * 4;
+            const int box = cc / C::OBW, cin = cc % C::OBW;
+            uint8_t* dst = stg + box * (128 * C::OSW) + swz(r * C::OSW + cin * 4, C::OSW);
+            *(uint4*)dst = make_uint4(o[0], o[1], o[2], o[3]);
             uint32_t* zt = (uint32_t*)p.z + p.full_rows * (int64_t)W + h * C::FILLW + cc;
 #pragma unroll
             for (int e = 0; e < 4; ++e)
