@@ -1422,6 +1422,34 @@ __device__ __forceinline__ void seg_epilogue(const ScanParams& p, const CUtensor
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(&ctl->slot_empty[g][j]);
+      // warps whose rows hold no segment start and no ragged tail: y = z +
+      // carry (fp32 split: z * 2^-k + carry, fused), two columns per instruction
+      const bool plain = !sums_out && !__any_sync(0xffffffffu, mk != 0ull || is_tail);
+      if (plain) {
+#pragma unroll
+        for (int e4 = 0; e4 < W / 4; ++e4) {
+          uint4 o;
+          const uint32_t* ve = &v[e4 * 4];
+          if constexpr (IS_INT) {
+            o = make_uint4(ve[0] + ci, ve[1] + ci, ve[2] + ci, ve[3] + ci);
+          } else {
+            const f32x2_t c2 = f2_make(cf, cf);
+            f32x2_t a = f2_bits(ve[0], ve[1]), b = f2_bits(ve[2], ve[3]);
+            if constexpr (C::F16SPLIT) {
+              const f32x2_t s2 = f2_make(rsv[j], rsv[j]);
+              a = f2_fma(a, s2, c2);
+              b = f2_fma(b, s2, c2);
+            } else {
+              a = f2_add(a, c2);
+              b = f2_add(b, c2);
+            }
+            o = make_uint4((uint32_t)a, (uint32_t)(a >> 32), (uint32_t)b, (uint32_t)(b >> 32));
+          }
+          const int cc = e4 * 4;
+          const int box = cc / C::OBW, cin = cc % C::OBW;
+          *(uint4*)(stg + box * (128 * C::OSW) + swz(r * C::OSW + cin * 4, C::OSW)) = o;
+        }
+      } else {
       if constexpr (C::F16SPLIT) {  // undo the row's operand scale (a power of two: exact)
 #pragma unroll
         for (int c = 0; c < W; ++c) v[c] = __float_as_uint(__uint_as_float(v[c]) * rsv[j]);
@@ -1476,6 +1504,7 @@ __device__ __forceinline__ void seg_epilogue(const ScanParams& p, const CUtensor
               if (cc + e < p.tail) zt[e] = o[e];
           }
         }
+      }
       }
       fence_proxy_async_smem();
       named_bar_sync(bar_id, 128);
