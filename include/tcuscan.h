@@ -226,15 +226,16 @@ TCU_API tcu_status_t tcu_seg_bounds(const void* x, tcu_dtype_t x_dtype, int64_t 
 TCU_API tcu_status_t tcu_spmv_csr(const void* vals, tcu_dtype_t dtype, const void* indptr, tcu_dtype_t indptr_dtype,
                                   int64_t rows, const int32_t* cols, int64_t nnz, const void* x, int64_t x_len, int S,
                                   float* y, float* prod_tmp, void* ws, size_t ws_bytes, void* stream);
-/* Segment sums and SpMV split by elements on the SIMT cores (bound by HBM
- * for any mix of segment lengths, where the tensor-core segmented sum is
- * bound by segment starts when segments are short): 4096 elements per CTA,
- * 16 consecutive per thread, rows crossing threads combined by a segmented
- * scan and rows crossing CTAs by an in-order fix-up, so each segment is
- * summed in a fixed order (FP32 for fp16 / fp32 input, exact int32 for
- * int8), independent of the launch.  Empty segments give 0.  ws: a
- * workspace of at least tcu_rows_workspace_bytes(n) bytes (its scratch is
- * zeroed again before the call returns).
+/* Segment sums and SpMV split by elements on the SIMT cores (the
+ * tensor-core segmented sum is bound by segment starts when segments are
+ * short): 128 bytes of input per thread (32 elements for SpMV), segment
+ * starts and ends marked in per-tile bitmaps, segments crossing threads
+ * combined by a segmented scan and segments crossing CTAs by an in-order
+ * fix-up, so each segment is summed in a fixed order (FP32 for fp16 / fp32
+ * input, exact int32 for int8), independent of the launch.  Bounds must be
+ * non-decreasing; empty segments give 0.  ws: a workspace of at least
+ * tcu_rows_workspace_bytes(n) bytes (its scratch is zeroed again before the
+ * call returns).
  * tcu_seg_sum_rows: out[k] = sum x[bounds[k]:bounds[k+1]] (bounds clamped to
  * [0, n]) -- the out_sums form of tcu_seg_bounds.
  * tcu_spmv_rows: y = A x with fp32 products vals[i] * x[cols[i]]; columns

@@ -2,27 +2,37 @@
 //
 // Reference: run_seg_sum_multi_core (src/torch/torch_seg_ops.h:333-426) and
 // run_spmv_v2 (src/torch/torch_spmv.h:112-209) sum each CSR row with the
-// matrix-unit scan and a per-segment revert walk.  The tensor-core segmented
-// sum here (scan_tc_kernel<..., kSegBounds>) is bound by segment starts when
-// rows are short (an SpMV row of 16 nonzeros gives ~2000 starts per 32768-
-// element tile).  A segment SUM needs no prefix output, so this path splits
-// the elements -- not the rows -- evenly and stays bound by HBM for any mix
-// of row lengths:
-//   nz_rowrange_kernel   one warp per tile of 4096 elements: the row holding
-//                        the tile's first element (a 32-way search of the
-//                        bounds, four rounds for 2^20 rows);
-//   nz_split_kernel      one CTA per tile, 16 consecutive elements per thread
-//                        (16-byte loads; SpMV gathers x from L2 and multiplies
-//                        in FP32).  Each thread sums its elements in order and
-//                        writes every row that starts and ends inside its 16;
-//                        a row that crosses threads is finished by the thread
-//                        where it ends, with the partial sums of the threads
-//                        before it from one segmented scan over the CTA; a row
-//                        that crosses tiles leaves its partial sums per tile;
-//   nz_fixup_kernel      one thread per tile whose first row started in an
-//                        earlier tile adds those partials in tile order.
-// Every row is summed in a fixed order, so results do not depend on the
-// launch.  Empty rows are zeroed up front.  No kernel waits on another CTA.
+// matrix-unit scan and a per-segment revert walk.  A segment SUM needs no
+// prefix output, so this path splits the elements -- not the segments --
+// evenly and marks the segment boundaries in per-tile bitmaps, which keeps
+// every element's work to a few branch-free instructions for any mix of
+// segment lengths:
+//   bm_tile_first_kernel  one warp per tile: the first bound at or after the
+//                         tile start (a 32-way search);
+//   bm_segsum_kernel      one CTA per tile, 128 bytes of input per thread
+//                         (32 elements for SpMV: it gathers x[cols] and
+//                         multiplies in FP32), loads issued first.  The
+//                         tile's bounds set two bitmaps in shared memory, one
+//                         bit per element: segment starts and segment ends
+//                         (the last element of every non-empty segment).
+//                         Each thread takes its elements 32 at a time: their
+//                         inclusive prefix P goes to the thread's padded row
+//                         of shared memory, and every end e, visited by bit,
+//                         gets P[e] - P[s - 1] for the last start s <= e (or
+//                         P[e] plus the sum carried in from before).  An end's
+//                         output index is the tile's first segment index plus
+//                         the end's ordinal (a popcount prefix of the end
+//                         bitmap) -- or, in a tile whose bounds hold an empty
+//                         segment, a search of the tile's bounds.  Threads
+//                         are chained by one segmented scan of their tails;
+//                         empty segments get 0 from the tile holding their
+//                         bound;
+//   bm_fixup_kernel       one thread per tile whose first end closes a segment
+//                         that began in an earlier tile: adds the tails of the
+//                         tiles before it, in tile order, in FP64.
+// Every segment is summed in a fixed order, so results do not depend on the
+// launch, and no kernel waits on another CTA.  Bounds must be non-decreasing
+// (values are clamped to [0, n]).
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
@@ -30,10 +40,18 @@
 
 namespace tcu {
 
-constexpr int kNzThreads = 256;
-constexpr int kNzWarps = kNzThreads / 32;
-constexpr int kNzTile = kNzThreads * 16;  // the smallest tile (SpMV): workspace sizing
-constexpr int kNzStageCap = 4096 + 2;      // row starts staged in shared memory per tile
+constexpr int kBmThreads = 256;
+constexpr int kBmWarps = kBmThreads / 32;
+// Elements per thread: 128 bytes of input (32 for SpMV, whose products take
+// a register each), so a CTA moves 32 KB per tile.  The boundary bitmaps
+// give every element one bit: thread t owns words [t * IPT / 32, ...).
+template <typename VT, bool SPMV>
+struct BmCfg {
+  static constexpr int IPT = SPMV ? 32 : 128 / (int)sizeof(VT);
+  static constexpr int WPT = IPT / 32;  // bitmap words per thread
+  static constexpr int TILE = kBmThreads * IPT;
+};
+constexpr int kBmMinTile = kBmThreads * 32;  // the smallest tile (workspace sizing)
 
 template <typename T>
 __device__ __forceinline__ float elem_f32(const T* p);
@@ -48,187 +66,139 @@ __device__ __forceinline__ int64_t bound_at(const IT* b, int64_t i, int64_t n) {
   return v < 0 ? 0 : (v > n ? n : v);
 }
 
-// Rows are numbered internally ri = 0 .. nseg + 1: ri = 0 holds the elements
-// before bounds[0], ri = 1 .. nseg are the segments, ri = nseg + 1 holds the
-// elements from bounds[nseg] on; only 1 .. nseg are written (out[ri - 1]).
-// row_start(ri) for ri in [0, nseg + 2].
-template <typename IT>
-__device__ __forceinline__ int64_t row_start(const IT* b, int64_t ri, int64_t nseg, int64_t n) {
-  if (ri <= 0) return 0;
-  if (ri > nseg + 1) return n;
-  return bound_at(b, ri - 1, n);
-}
-
-// Per-tile carries, in the caller's workspace scratch.
-template <typename ACC>
-struct NzCarry {
-  long long head_row;  // internal id of the tile's first row if it began in an earlier tile and ends here, else -1
-  long long tail_row;  // internal id of the row that continues past the tile's end, else -1
-  ACC head_val;        // this tile's part of head_row
-  ACC tail_val;        // this tile's part of tail_row (the whole tile when span)
-  int span;            // the tile lies inside one row that continues on both sides
+// Per-tile record for the cross-tile fix-up (CT: FP64 for floating sums,
+// int32 for int8 sums).
+template <typename CT>
+struct BmCarry {
+  CT tail;           // sum of the tile's elements after its last segment start (the whole tile without one)
+  long long head_k;  // output index of the tile's first segment end when that segment began earlier, else -1
+  int has_start;     // the tile holds a segment start
+  int pad;
 };
 
-// The internal row holding the first element of each tile: the largest ri in
-// [0, nseg + 1] with row_start(ri) <= tile start (bounds assumed
-// non-decreasing; any bounds keep every access in range).
+// tile_first[c] = first index i in [0, nb] with clamp(bounds[i]) >= c * tile,
+// for c in [0, tiles); tile_first[tiles] = nb.  One warp per entry.
 template <typename IT>
-__global__ void __launch_bounds__(256) nz_rowrange_kernel(const IT* __restrict__ bounds, int64_t nseg, int64_t n,
-                                                          int64_t tiles, int tile, long long* __restrict__ row_lo) {
+__global__ void __launch_bounds__(256) bm_tile_first_kernel(const IT* __restrict__ bounds, int64_t nb, int64_t n,
+                                                            int64_t tiles, int tile, long long* __restrict__ tile_first) {
   const int lane = threadIdx.x & 31;
-  const int64_t t = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (t >= tiles) return;  // warp-uniform
-  const int64_t key = t * tile;
-  int64_t lo = 0, hi = nseg + 1;  // answer in [lo, hi]: row_start(lo) <= key
-  while (hi - lo > 31) {
+  const int64_t c = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (c > tiles) return;  // warp-uniform
+  if (c == tiles) {
+    if (lane == 0) tile_first[c] = nb;
+    return;
+  }
+  const int64_t key = c * tile;
+  int64_t lo = 0, hi = nb;  // the answer lies in [lo, hi]
+  while (hi - lo > 32) {
     const int64_t step = (hi - lo + 31) / 32;
     const int64_t p = lo + lane * step;
-    const bool ok = p <= hi && row_start(bounds, p, nseg, n) <= key;
-    const unsigned m = __ballot_sync(0xffffffffu, ok);  // lane 0 always true
-    const int L = 31 - __clz(m);
-    const int64_t nlo = lo + L * step;
-    const int64_t nhi = L == 31 ? hi : (lo + (L + 1) * step - 1 < hi ? lo + (L + 1) * step - 1 : hi);
+    const bool below = p < hi && bound_at(bounds, p, n) < key;
+    const int cnt = __popc(__ballot_sync(0xffffffffu, below));  // probes below the key: a prefix of the lanes
+    const int64_t nlo = cnt == 0 ? lo : lo + (int64_t)(cnt - 1) * step + 1;
+    const int64_t nhi = lo + (int64_t)cnt * step < hi ? lo + (int64_t)cnt * step : hi;
     lo = nlo;
     hi = nhi;
   }
   const int64_t p = lo + lane;
-  const bool ok = p <= hi && row_start(bounds, p, nseg, n) <= key;
-  const unsigned m = __ballot_sync(0xffffffffu, ok);
-  if (lane == 0) row_lo[t] = lo + (31 - __clz(m));
+  const bool below = p < hi && bound_at(bounds, p, n) < key;
+  const int cnt = __popc(__ballot_sync(0xffffffffu, below));
+  if (lane == 0) tile_first[c] = lo + cnt;
 }
 
-// Segmented inclusive scan over the CTA's threads: a thread with reset = 1
-// starts a new segment.  Returns the thread's inclusive value; `sv`/`sr` are
-// kNzWarps-entry scratch.
-template <typename ACC>
-__device__ __forceinline__ ACC block_seg_scan(ACC v, int reset, ACC* sv, int* sr) {
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  int r = reset;
-#pragma unroll
-  for (int d = 1; d < 32; d <<= 1) {
-    const ACC ov = __shfl_up_sync(0xffffffffu, v, d);
-    const int orr = __shfl_up_sync(0xffffffffu, r, d);
-    if (lane >= d) {
-      if (!r) v += ov;
-      r |= orr;
-    }
+// First index in [lo, hi) with clamp(bounds[i]) >= key (hi if none).
+template <typename IT>
+__device__ __forceinline__ int64_t bm_lower_bound(const IT* bounds, int64_t lo, int64_t hi, int64_t key, int64_t n) {
+  while (lo < hi) {
+    const int64_t mid = lo + ((hi - lo) >> 1);
+    if (bound_at(bounds, mid, n) < key) lo = mid + 1;
+    else hi = mid;
   }
-  if (lane == 31) {
-    sv[w] = v;
-    sr[w] = r;
-  }
-  __syncthreads();
-  if (!r) {  // no reset in this warp up to this lane: add the warps before, back to the last reset
-    for (int k = w - 1; k >= 0; --k) {
-      v += sv[k];
-      if (sr[k]) break;
-    }
-  }
-  __syncthreads();
-  return v;
+  return lo;
 }
 
-// VT: element type; ACC: accumulator / output type; SPMV: element i is
-// vals[i] * x[cols[i]] (FP32 product), else vals[i].  Segment r covers
-// [bounds[r], bounds[r + 1]) (clamped); the tiles cover all n elements.
-template <typename VT, typename ACC, bool SPMV, typename IT, int ITEMS>
-__global__ void __launch_bounds__(kNzThreads, 4) nz_split_kernel(const VT* __restrict__ vals,
-                                                              const int32_t* __restrict__ cols,
-                                                              const VT* __restrict__ x, int64_t x_len,
-                                                              const IT* __restrict__ bounds, int64_t nseg, int64_t n,
-                                                              const long long* __restrict__ row_lo,
-                                                              ACC* __restrict__ out, NzCarry<ACC>* __restrict__ carry,
-                                                              WsHeader* ws) {
-  constexpr int TILE = kNzThreads * ITEMS;
-  __shared__ ACC sv[kNzWarps];
-  __shared__ int sr[kNzWarps];
+// VT: element type; ACC: per-tile accumulator and output type (FP32, or
+// int32 for int8); CT: cross-tile carry type; SPMV: element i is
+// vals[i] * x[cols[i]] (FP32 product), else vals[i].
+template <typename VT, typename ACC, typename CT, bool SPMV, typename IT>
+__global__ void __launch_bounds__(kBmThreads, SPMV ? 3 : 4) bm_segsum_kernel(const VT* __restrict__ vals,
+                                                                  const int32_t* __restrict__ cols,
+                                                                  const VT* __restrict__ x, int64_t x_len,
+                                                                  const IT* __restrict__ bounds, int64_t nb,
+                                                                  int64_t n, const long long* __restrict__ tile_first,
+                                                                  ACC* __restrict__ out, BmCarry<CT>* __restrict__ carry,
+                                                                  WsHeader* ws) {
+  using C = BmCfg<VT, SPMV>;
+  constexpr int IPT = C::IPT, WPT = C::WPT, TILE = C::TILE;
+  __shared__ uint32_t sS[kBmThreads * WPT];  // segment-start bits
+  __shared__ uint32_t sE[kBmThreads * WPT];  // segment-end bits (the last element of every non-empty segment)
+  __shared__ ACC swv[kBmWarps];
+  __shared__ int swf[kBmWarps], swc[kBmWarps];
+  __shared__ __align__(16) ACC sP[kBmThreads * 36];  // per-thread word prefixes (row of 36)
+  __shared__ unsigned long long s_kfirst;  // output index of the tile's first end
+  __shared__ int s_empty;                  // the tile's bounds hold an empty segment
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
   const int64_t c = blockIdx.x;
-  const int64_t t_lo = c * TILE;
-  const int64_t t_hi = t_lo + TILE < n ? t_lo + TILE : n;
-  const int64_t j0 = t_lo + (int64_t)threadIdx.x * ITEMS;
-  const int64_t j_end = j0 + ITEMS < t_hi ? j0 + ITEMS : t_hi;  // this thread's [j0, j_end)
-  const bool has_items = j0 < t_hi;
-  const int64_t r_tile = row_lo[c];
-  const int64_t r_last = c + 1 < gridDim.x ? row_lo[c + 1] : nseg + 1;  // rows of this tile lie in [r_tile, r_last]
+  const int64_t t0 = c * TILE;
+  const int64_t t1 = t0 + TILE < n ? t0 + TILE : n;
+  const int64_t j0 = t0 + (int64_t)t * IPT;
+  const int nvalid = j0 >= t1 ? 0 : (j0 + IPT <= t1 ? IPT : (int)(t1 - j0));
 
-  // ---- the thread's elements: SpMV products, or the packed input words ----
-  const bool full = j0 + ITEMS <= t_hi;
-  const bool vec_v = full && ((reinterpret_cast<uintptr_t>(vals + j0) & 15u) == 0);
-  constexpr int WORDS = SPMV ? 1 : ITEMS * (int)sizeof(VT) / 4;
-  float p[SPMV ? ITEMS : 1];
+  // ---- the thread's elements: loads issued before the bounds work ----
+  constexpr int WORDS = SPMV ? 1 : IPT * (int)sizeof(VT) / 4;
   uint32_t raw[WORDS];
+  int32_t cc[SPMV ? IPT : 1];
+  float pv[SPMV ? IPT : 1];
+  const bool vec = nvalid == IPT && ((reinterpret_cast<uintptr_t>(vals) & 15u) == 0) &&
+                   (!SPMV || (reinterpret_cast<uintptr_t>(cols) & 15u) == 0);
   if constexpr (SPMV) {
-    // Coalesced: lane L of warp w loads elements w*512 + q*128 + 4L .. +3
-    // (q = 0..3), so every load instruction covers whole 128-byte lines; the
-    // products then go through padded shared memory (16 bytes of padding per
-    // 32 products: conflict-free both ways) into each thread's 16
-    // consecutive elements, the order the row logic below needs.
-    static_assert(ITEMS == 16, "the SpMV transpose assumes 16 elements per thread");
-    __shared__ __align__(16) float s_prod[kNzWarps][512 + 64];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int64_t wbase = t_lo + (int64_t)w * 512;
-    const bool aligned = ((reinterpret_cast<uintptr_t>(cols) | reinterpret_cast<uintptr_t>(vals)) & 15u) == 0 &&
-                         (sizeof(VT) == 4 || (reinterpret_cast<uintptr_t>(vals) & 7u) == 0);
+    if (vec) {
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int64_t e0 = wbase + q * 128 + 4 * lane;
-      int32_t cc[4];
-      float va[4];
-      if (aligned && e0 + 4 <= t_hi) {
-        const int4 c4 = __ldg(reinterpret_cast<const int4*>(cols + e0));
-        cc[0] = c4.x; cc[1] = c4.y; cc[2] = c4.z; cc[3] = c4.w;
-        if constexpr (sizeof(VT) == 4) {
-          const float4 v4 = __ldg(reinterpret_cast<const float4*>(vals + e0));
-          va[0] = v4.x; va[1] = v4.y; va[2] = v4.z; va[3] = v4.w;
-        } else {
-          const uint2 u = __ldg(reinterpret_cast<const uint2*>(vals + e0));
-          const float2 f0 = __half22float2(*reinterpret_cast<const __half2*>(&u.x));
-          const float2 f1 = __half22float2(*reinterpret_cast<const __half2*>(&u.y));
-          va[0] = f0.x; va[1] = f0.y; va[2] = f1.x; va[3] = f1.y;
+      for (int q = 0; q < IPT / 4; ++q) {
+        const int4 c4 = __ldg(reinterpret_cast<const int4*>(cols + j0) + q);
+        cc[4 * q] = c4.x; cc[4 * q + 1] = c4.y; cc[4 * q + 2] = c4.z; cc[4 * q + 3] = c4.w;
+      }
+      if constexpr (sizeof(VT) == 4) {
+#pragma unroll
+        for (int q = 0; q < IPT / 4; ++q) {
+          const float4 v4 = __ldg(reinterpret_cast<const float4*>(vals + j0) + q);
+          pv[4 * q] = v4.x; pv[4 * q + 1] = v4.y; pv[4 * q + 2] = v4.z; pv[4 * q + 3] = v4.w;
         }
       } else {
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          const bool in = e0 + i < t_hi;
-          cc[i] = in ? __ldg(cols + e0 + i) : 0;
-          va[i] = in ? elem_f32<VT>(vals + e0 + i) : 0.f;
+        for (int q = 0; q < IPT / 8; ++q) {
+          const uint4 u = __ldg(reinterpret_cast<const uint4*>(vals + j0) + q);
+          const uint32_t uu[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+          for (int h = 0; h < 4; ++h) {
+            const float2 f = __half22float2(*reinterpret_cast<const __half2*>(&uu[h]));
+            pv[8 * q + 2 * h] = f.x;
+            pv[8 * q + 2 * h + 1] = f.y;
+          }
         }
       }
-      float pr[4];
+    } else {
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        float xv = 0.f;
-        if ((unsigned long long)(unsigned)cc[i] < (unsigned long long)x_len) xv = elem_f32<VT>(x + cc[i]);
-        else if (e0 + i < t_hi && ws) record_error(ws, TCU_ERR_ARG, 301, (uint32_t)(e0 + i));
-        pr[i] = __fmul_rn(va[i], xv);
+      for (int i = 0; i < IPT; ++i) {
+        const bool in = i < nvalid;
+        cc[i] = in ? __ldg(cols + j0 + i) : 0;
+        pv[i] = in ? elem_f32<VT>(vals + j0 + i) : 0.f;
       }
-      const int el = q * 128 + 4 * lane;  // element within the warp's 512
-      *reinterpret_cast<float4*>(&s_prod[w][el + (el >> 5) * 4]) = make_float4(pr[0], pr[1], pr[2], pr[3]);
-    }
-    __syncwarp();
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      const int el = 16 * lane + 4 * c;
-      const float4 f = *reinterpret_cast<const float4*>(&s_prod[w][el + (el >> 5) * 4]);
-      p[4 * c] = f.x; p[4 * c + 1] = f.y; p[4 * c + 2] = f.z; p[4 * c + 3] = f.w;
     }
   } else {
-    if (vec_v) {
+    if (vec) {
 #pragma unroll
       for (int q = 0; q < WORDS / 4; ++q) {
         const uint4 u = __ldg(reinterpret_cast<const uint4*>(vals + j0) + q);
-        raw[4 * q] = u.x;
-        raw[4 * q + 1] = u.y;
-        raw[4 * q + 2] = u.z;
-        raw[4 * q + 3] = u.w;
+        raw[4 * q] = u.x; raw[4 * q + 1] = u.y; raw[4 * q + 2] = u.z; raw[4 * q + 3] = u.w;
       }
-    } else {  // ragged or unaligned: element by element, packed the same way
+    } else {  // ragged or unaligned: element by element, packed the same way (zeros past the end)
 #pragma unroll
-      for (int w = 0; w < WORDS; ++w) raw[w] = 0;
+      for (int q = 0; q < WORDS; ++q) raw[q] = 0;
       const uint8_t* vb = reinterpret_cast<const uint8_t*>(vals + j0);
 #pragma unroll
-      for (int i = 0; i < ITEMS; ++i) {
-        if (j0 + i < t_hi) {
+      for (int i = 0; i < IPT; ++i) {
+        if (i < nvalid) {
           uint32_t bits;
           if constexpr (sizeof(VT) == 1) bits = vb[i];
           else if constexpr (sizeof(VT) == 2) bits = reinterpret_cast<const uint16_t*>(vb)[i];
@@ -238,10 +208,75 @@ __global__ void __launch_bounds__(kNzThreads, 4) nz_split_kernel(const VT* __res
       }
     }
   }
-  // element i of the thread as ACC (constant i after unrolling)
+
+  // ---- boundary bitmaps from the tile's bounds ----
+#pragma unroll
+  for (int q = 0; q < WPT; ++q) {
+    sS[t * WPT + q] = 0u;
+    sE[t * WPT + q] = 0u;
+  }
+  if (t == 0) {
+    s_kfirst = ~0ull;
+    s_empty = 0;
+  }
+  __syncthreads();
+  const int64_t i_lo = tile_first[c];
+  const int64_t i_own = tile_first[c + 1];            // bounds [i_lo, i_own) lie in [t0, t1) (the last tile: [t0, n])
+  const int64_t i_end = i_own < nb ? i_own + 1 : nb;  // + the first later bound: it may end a segment at t1 - 1
+  for (int64_t i = i_lo + t; i < i_end; i += kBmThreads) {
+    const int64_t b = bound_at(bounds, i, n);
+    const int64_t bp = i >= 1 ? bound_at(bounds, i - 1, n) : -1;
+    if (i < i_own) {
+      if (b >= t0 && b < t1) atomicOr(&sS[(b - t0) >> 5], 1u << ((b - t0) & 31));
+      if (i >= 1 && b == bp) {  // an empty segment
+        out[i - 1] = ACC(0);
+        s_empty = 1;
+      }
+    }
+    if (i >= 1 && b > bp && b - 1 >= t0 && b - 1 < t1) {  // segment i - 1 ends at b - 1, in this tile
+      const int64_t e = b - 1 - t0;
+      atomicOr(&sE[e >> 5], 1u << (e & 31));
+      atomicMin(&s_kfirst, (unsigned long long)(i - 1));
+    }
+  }
+  __syncthreads();
+  uint32_t Sw[WPT], Ew[WPT];
+  int ec = 0;
+#pragma unroll
+  for (int q = 0; q < WPT; ++q) {
+    Sw[q] = sS[t * WPT + q];
+    Ew[q] = sE[t * WPT + q];
+    ec += __popc(Ew[q]);
+  }
+  // ends before this thread's words: block exclusive scan of the popcounts
+  int ecs = ec;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const int o = __shfl_up_sync(0xffffffffu, ecs, d);
+    if (lane >= d) ecs += o;
+  }
+  if (lane == 31) swc[w] = ecs;
+  const int64_t kfirst = (int64_t)s_kfirst;  // read before the barrier below
+  const bool direct = s_empty == 0;          // no empty segment: the ends' outputs are consecutive
+  __syncthreads();
+  int wpre = 0;
+#pragma unroll
+  for (int k = 0; k < kBmWarps; ++k) wpre += k < w ? swc[k] : 0;
+  int ord = wpre + ecs - ec;
+
+  // ---- SpMV: gather x[cols] (FP32 products) ----
+  if constexpr (SPMV) {
+#pragma unroll
+    for (int i = 0; i < IPT; ++i) {
+      float xv = 0.f;
+      if ((unsigned long long)(unsigned)cc[i] < (unsigned long long)x_len) xv = elem_f32<VT>(x + cc[i]);
+      else if (i < nvalid && ws) record_error(ws, TCU_ERR_ARG, 301, (uint32_t)(j0 + i));
+      pv[i] = __fmul_rn(pv[i], xv);
+    }
+  }
   auto elem = [&](int i) -> ACC {
     if constexpr (SPMV) {
-      return p[i];
+      return pv[i];
     } else if constexpr (sizeof(VT) == 1) {
       return (ACC)(int8_t)(raw[i >> 2] >> (8 * (i & 3)));
     } else if constexpr (sizeof(VT) == 2) {
@@ -250,202 +285,192 @@ __global__ void __launch_bounds__(kNzThreads, 4) nz_split_kernel(const VT* __res
       return (ACC)__uint_as_float(raw[i]);
     }
   };
-
-  // ---- fast path: the next tile's first element is in this tile's first row,
-  // so the whole tile lies in one row that goes on past it (block-uniform) ----
-  if (c + 1 < gridDim.x && r_tile == r_last) {
-    ACC part = (ACC)0;
-#pragma unroll
-    for (int i = 0; i < ITEMS; ++i) part += elem(i);  // every thread of this tile is full
-    part = warp_sum_any(part);
-    if ((threadIdx.x & 31) == 0) sv[threadIdx.x >> 5] = part;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      ACC tot = (ACC)0;
-#pragma unroll
-      for (int k = 0; k < kNzWarps; ++k) tot += sv[k];
-      const bool began_before = row_start(bounds, r_tile, nseg, n) < t_lo;
-      carry[c].head_row = -1;
-      carry[c].tail_row = r_tile;  // the row goes on into the next tile
-      carry[c].tail_val = tot;
-      carry[c].span = began_before ? 1 : 0;  // else the row begins here (a tail)
-    }
-    return;
-  }
-
-  // ---- the starts of the tile's rows [r_tile, r_last + 1], relative to the
-  // tile start and clamped to [-1, kNzTile + 1], staged in shared memory ----
-  __shared__ int s_st[kNzStageCap];
-  const int64_t cnt = r_last - r_tile + 2;
-  const bool staged = cnt <= kNzStageCap;  // block-uniform; else read from global memory
-  if (staged) {
-    for (int i = threadIdx.x; i < (int)cnt; i += kNzThreads) {
-      const int64_t v = row_start(bounds, r_tile + i, nseg, n) - t_lo;
-      s_st[i] = v < -1 ? -1 : (v > TILE ? TILE + 1 : (int)v);
-    }
-  }
-  __syncthreads();
-  auto S = [&](int64_t ri) -> int {
-    const int64_t k = ri - r_tile;
-    if (staged) return k < 0 ? -1 : (k < cnt ? s_st[k] : TILE + 1);
-    const int64_t v = row_start(bounds, ri, nseg, n) - t_lo;
-    return v < -1 ? -1 : (v > TILE ? TILE + 1 : (int)v);
+  // output index of the end with ordinal o at tile element e
+  auto out_index = [&](int o, int e) -> int64_t {
+    if (direct) return kfirst + o;
+    return bm_lower_bound(bounds, i_lo, i_end, t0 + e + 1, n) - 1;
   };
-  const int j0r = (int)(j0 - t_lo), j_endr = (int)(j_end - t_lo);  // tile-relative
 
-  // ---- the thread's first row: largest ri in [r_tile, r_last] with start <= j0 ----
-  int64_t row = r_tile;
-  if (has_items) {
-    int64_t lo = r_tile, hi = r_last;
-    while (lo < hi) {
-      const int64_t mid = (lo + hi + 1) >> 1;
-      if (S(mid) <= j0r) lo = mid;
-      else hi = mid - 1;
-    }
-    row = lo;
-  }
-  const int row_begin = S(row);
-  const bool tile_head_row = has_items && row_begin < 0;  // the thread's first row began before the tile
-  bool head_open = has_items && row_begin < j0r;          // it began before this thread
-  const int64_t head_row = row;
-  ACC head_val = (ACC)0;
-  bool has_head = false;
-  ACC acc = (ACC)0;
-  int next = has_items ? S(row + 1) : 0;
-  if (has_items) {
+  // ---- the thread's segmented sums, a word (32 elements) at a time: the
+  // word's inclusive prefix P goes to the thread's row of shared memory
+  // (36 entries: rows 144 bytes apart, so the 16-byte stores of 8 lanes hit
+  // distinct banks), then every end e takes P[e] - P[s - 1] for the last
+  // start s <= e in the word, or P[e] plus the sum carried in from before
+  // the word.  No per-element branch: the ends are visited by bit. ----
+  ACC* myP = sP + t * 36;
+  ACC running = ACC(0);  // sum since the thread's last start (everything so far without one)
+  bool open = true;      // no start seen yet in this thread
+  int open_ord = -1, open_e = 0;
+  ACC open_val = ACC(0);
 #pragma unroll
-    for (int i = 0; i < ITEMS; ++i) {
-      const int j = j0r + i;
-      if (j < j_endr) {
-        while (next <= j) {  // the current row ends before element j (empty rows pass through)
-          if (head_open) {
-            has_head = true;
-            head_val = acc;
-            head_open = false;
-          } else if (row >= 1 && row <= nseg) {
-            out[row - 1] = acc;
-          }
-          acc = (ACC)0;
-          ++row;
-          next = S(row + 1);
+  for (int q = 0; q < WPT; ++q) {
+    const uint32_t sw = Sw[q];
+    uint32_t em = Ew[q];
+    const bool need = (sw | em) != 0u;
+    ACC pfx = ACC(0);
+#pragma unroll
+    for (int i4 = 0; i4 < 8; ++i4) {
+      const ACC a0 = pfx + elem(q * 32 + 4 * i4);
+      const ACC a1 = a0 + elem(q * 32 + 4 * i4 + 1);
+      const ACC a2 = a1 + elem(q * 32 + 4 * i4 + 2);
+      const ACC a3 = a2 + elem(q * 32 + 4 * i4 + 3);
+      if (need) {
+        if constexpr (sizeof(ACC) == 4) {
+          uint4 u;
+          u.x = *reinterpret_cast<const uint32_t*>(&a0);
+          u.y = *reinterpret_cast<const uint32_t*>(&a1);
+          u.z = *reinterpret_cast<const uint32_t*>(&a2);
+          u.w = *reinterpret_cast<const uint32_t*>(&a3);
+          *reinterpret_cast<uint4*>(myP + 4 * i4) = u;
         }
-        acc += elem(i);
       }
+      pfx = a3;
     }
-  }
-  // the last row: ends exactly at j_end, or continues past it
-  bool carry_out = false, span = false;
-  if (has_items) {
-    if (next == j_endr) {
-      if (head_open) {
-        has_head = true;
-        head_val = acc;
-        head_open = false;
-      } else if (row >= 1 && row <= nseg) {
-        out[row - 1] = acc;
+    while (em) {
+      const int i = __ffs(em) - 1;
+      em &= em - 1u;
+      const uint32_t sb = sw & (0xFFFFFFFFu >> (31 - i));  // starts at or before i
+      const ACC pe = myP[i];
+      const int e = t * IPT + q * 32 + i;
+      if (sb) {
+        const int ls = 31 - __clz(sb);
+        out[out_index(ord, e)] = pe - (ls ? myP[ls - 1] : ACC(0));
+      } else if (!open) {
+        out[out_index(ord, e)] = running + pe;
+      } else {  // the segment began before this thread: finished after the carry scan
+        open_ord = ord;
+        open_e = e;
+        open_val = running + pe;
       }
+      ++ord;
+    }
+    if (sw) {
+      const int ls = 31 - __clz(sw);
+      running = pfx - (ls ? myP[ls - 1] : ACC(0));
+      open = false;
     } else {
-      carry_out = true;
-      span = head_open;  // inside one row from the thread's first element to its last
+      running += pfx;
     }
   }
-  // partial sums of rows crossing threads: segmented scan, a segment per starting row
-  const ACC scanned = block_seg_scan<ACC>(carry_out ? acc : (ACC)0, carry_out ? (span ? 0 : 1) : 1, sv, sr);
-  // carry into this thread's head row = the previous thread's scanned value
-  const ACC carry_in = __shfl_up_sync(0xffffffffu, scanned, 1);
-  __shared__ ACC s_last[kNzWarps];
-  if ((threadIdx.x & 31) == 31) s_last[threadIdx.x >> 5] = scanned;
-  __syncthreads();
-  const ACC prev = (threadIdx.x & 31) ? carry_in : (threadIdx.x ? s_last[(threadIdx.x >> 5) - 1] : (ACC)0);
-  const int t_last = (int)((t_hi - t_lo - 1) / ITEMS);
-  if (threadIdx.x == 0) {
-    carry[c].head_row = -1;
-    carry[c].span = 0;
-  }
-  __syncthreads();
-  if (has_head) {
-    const ACC v = (threadIdx.x ? prev : (ACC)0) + head_val;
-    if (tile_head_row) {  // began in an earlier tile: the fix-up adds the earlier tiles' parts
-      carry[c].head_row = head_row;
-      carry[c].head_val = v;
-    } else if (head_row >= 1 && head_row <= nseg) {
-      out[head_row - 1] = v;
+  const ACC acc = running;
+  // ---- carries between threads: segmented scan of the threads' tails ----
+  ACC v = acc;  // the sum after this thread's last start (all of it without one)
+  int f = 0;
+#pragma unroll
+  for (int q = 0; q < WPT; ++q) f |= Sw[q] != 0u;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const ACC ov = __shfl_up_sync(0xffffffffu, v, d);
+    const int of = __shfl_up_sync(0xffffffffu, f, d);
+    if (lane >= d) {
+      if (!f) v += ov;
+      f |= of;
     }
   }
-  if ((int)threadIdx.x == t_last) {
-    carry[c].tail_row = carry_out ? row : -1;
-    carry[c].tail_val = scanned;
-    // the whole tile inside one row that began earlier and goes on
-    carry[c].span = (carry_out && span && S(row) < 0) ? 1 : 0;
+  if (lane == 31) {
+    swv[w] = v;
+    swf[w] = f;
   }
+  __syncthreads();
+  ACC pv_w = ACC(0);  // the warps before this one, back to the last start
+  int pf_w = 0;
+  for (int k = w - 1; k >= 0; --k) {
+    pv_w += swv[k];
+    if (swf[k]) {
+      pf_w = 1;
+      break;
+    }
+  }
+  const ACC vi = f ? v : pv_w + v;  // inclusive over the tile's threads
+  const int fi = f | pf_w;
+  ACC ve = __shfl_up_sync(0xffffffffu, vi, 1);
+  int fe = __shfl_up_sync(0xffffffffu, fi, 1);
+  if (lane == 0) {
+    ve = pv_w;
+    fe = pf_w;
+  }
+  if (t == kBmThreads - 1) {
+    carry[c].tail = (CT)vi;
+    carry[c].has_start = fi;
+  }
+  long long head_k = -1;
+  if (open_ord >= 0) {
+    const int64_t k = out_index(open_ord, open_e);
+    out[k] = open_val + ve;
+    if (!fe) head_k = k;  // no start before it in the tile: the tile's first end, finished by the fix-up
+  }
+  // the tile's first end is in the first thread holding an end; exactly one
+  // thread writes head_k (the value, or -1)
+  if (ord > 0 && ord - ec == 0 && ec > 0) carry[c].head_k = head_k;
+  if (t == kBmThreads - 1 && ord == 0) carry[c].head_k = -1;  // no end in the tile
 }
 
-// One thread per tile: a tile whose head row began in an earlier tile adds
-// the parts of the tiles before it (back to the tile where the row began).
-template <typename ACC>
-__global__ void __launch_bounds__(256) nz_fixup_kernel(const NzCarry<ACC>* __restrict__ carry, int64_t tiles,
-                                                       int64_t nseg, ACC* __restrict__ out) {
+// One thread per tile: a tile whose first end closes a segment that began in
+// an earlier tile adds the tails of the tiles before it (back to the tile
+// holding the segment's start), in tile order.
+template <typename ACC, typename CT>
+__global__ void __launch_bounds__(256) bm_fixup_kernel(const BmCarry<CT>* __restrict__ carry, int64_t tiles,
+                                                       ACC* __restrict__ out) {
   const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= tiles) return;
-  const long long r = carry[c].head_row;
-  if (r < 1 || r > nseg) return;  // none, or a range outside the segments
-  ACC total = carry[c].head_val;
-  for (int64_t k = c - 1; k >= 0; --k) {
-    if (carry[k].tail_row != r) break;
-    total += carry[k].tail_val;
-    if (!carry[k].span) break;
+  const long long k = carry[c].head_k;
+  if (k < 0) return;
+  CT tot = CT(0);
+  for (int64_t q = c - 1; q >= 0; --q) {
+    tot += carry[q].tail;
+    if (carry[q].has_start) break;
   }
-  out[r - 1] = total;
+  out[k] = (ACC)((CT)out[k] + tot);
 }
 
-// Scratch in the workspace's descriptor region: row_lo[tiles + 1], then the
-// per-tile carries (64-byte aligned).
-static size_t nz_scratch_bytes(int64_t tiles) {
-  return (size_t)(tiles + 1) * 8 + 64 + (size_t)tiles * sizeof(NzCarry<double>);
+// Scratch in the workspace's descriptor region: tile_first[tiles + 1], then
+// the per-tile carries (64-byte aligned).
+static size_t bm_scratch_bytes(int64_t tiles) {  // tiles of kBmMinTile elements or more
+  return (size_t)(tiles + 1) * 8 + 64 + (size_t)tiles * sizeof(BmCarry<double>);
 }
 
-template <typename VT, typename ACC, bool SPMV, typename IT>
-static tcu_status_t nz_run(const VT* vals, const int32_t* cols, const VT* x, int64_t x_len, const IT* bounds,
-                           int64_t nseg, int64_t n, ACC* out, void* ws, size_t ws_bytes, cudaStream_t st) {
-  cudaError_t e = cudaMemsetAsync(out, 0, (size_t)nseg * sizeof(ACC), st);  // empty rows
-  if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(row sums)");
-  if (n == 0) return TCU_OK;
-  // 16 elements per thread (64 per thread for sums -- 4x fewer tiles -- was
-  // measured no faster at 2^28 and slower for short segments)
-  constexpr int ITEMS = 16;
-  constexpr int TILE = kNzThreads * ITEMS;
+template <typename VT, typename ACC, typename CT, bool SPMV, typename IT>
+static tcu_status_t bm_run(const VT* vals, const int32_t* cols, const VT* x, int64_t x_len, const IT* bounds,
+                           int64_t nb, int64_t n, ACC* out, void* ws, size_t ws_bytes, cudaStream_t st) {
+  const int64_t nseg = nb - 1;
+  if (n == 0) {  // every segment is empty
+    cudaError_t e = cudaMemsetAsync(out, 0, (size_t)nseg * sizeof(ACC), st);
+    return e == cudaSuccess ? TCU_OK : cuda_fail(e, "cudaMemsetAsync(segment sums)");
+  }
+  constexpr int TILE = BmCfg<VT, SPMV>::TILE;
   const int64_t tiles = (n + TILE - 1) / TILE;
   if (tiles > 0x7FFFFFFF) return TCU_ERR_ARG;
-  const size_t need = nz_scratch_bytes(tiles);
+  const size_t need = bm_scratch_bytes(tiles);
   if (!ws || ws_capacity(ws_bytes) * 16 < (int64_t)need) return TCU_ERR_WORKSPACE;
-  long long* row_lo = reinterpret_cast<long long*>(ws_descs(ws));
-  NzCarry<ACC>* carry = reinterpret_cast<NzCarry<ACC>*>(
-      (reinterpret_cast<uintptr_t>(row_lo + tiles + 1) + 63) & ~(uintptr_t)63);
+  long long* tile_first = reinterpret_cast<long long*>(ws_descs(ws));
+  BmCarry<CT>* carry = reinterpret_cast<BmCarry<CT>*>(
+      (reinterpret_cast<uintptr_t>(tile_first + tiles + 1) + 63) & ~(uintptr_t)63);
   WsHeader* h = static_cast<WsHeader*>(ws);
-  nz_rowrange_kernel<IT><<<(unsigned)((tiles * 32 + 255) / 256), 256, 0, st>>>(bounds, nseg, n, tiles, TILE, row_lo);
-  nz_split_kernel<VT, ACC, SPMV, IT, ITEMS><<<(unsigned)tiles, kNzThreads, 0, st>>>(vals, cols, x, x_len, bounds, nseg,
-                                                                                    n, row_lo, out, carry, h);
-  nz_fixup_kernel<ACC><<<(unsigned)((tiles + 255) / 256), 256, 0, st>>>(carry, tiles, nseg, out);
-  e = cudaGetLastError();
-  if (e != cudaSuccess) return cuda_fail(e, "nz_split launch");
+  bm_tile_first_kernel<IT><<<(unsigned)(((tiles + 1) * 32 + 255) / 256), 256, 0, st>>>(bounds, nb, n, tiles, TILE,
+                                                                                       tile_first);
+  bm_segsum_kernel<VT, ACC, CT, SPMV, IT><<<(unsigned)tiles, kBmThreads, 0, st>>>(vals, cols, x, x_len, bounds, nb, n,
+                                                                                  tile_first, out, carry, h);
+  bm_fixup_kernel<ACC, CT><<<(unsigned)((tiles + 255) / 256), 256, 0, st>>>(carry, tiles, out);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "segment sum launch");
   // the scratch lives in the look-back descriptor region, which must hold only
   // descriptors or zeros between launches
-  e = cudaMemsetAsync(row_lo, 0, need, st);
+  e = cudaMemsetAsync(tile_first, 0, need, st);
   return e == cudaSuccess ? TCU_OK : cuda_fail(e, "cudaMemsetAsync(row scratch)");
 }
 
-template <typename VT, typename ACC, bool SPMV>
-static tcu_status_t nz_dispatch(const VT* vals, const int32_t* cols, const VT* x, int64_t x_len, const void* bounds,
-                                tcu_dtype_t bdt, int64_t nseg, int64_t n, ACC* out, void* ws, size_t ws_bytes,
+template <typename VT, typename ACC, typename CT, bool SPMV>
+static tcu_status_t bm_dispatch(const VT* vals, const int32_t* cols, const VT* x, int64_t x_len, const void* bounds,
+                                tcu_dtype_t bdt, int64_t nb, int64_t n, ACC* out, void* ws, size_t ws_bytes,
                                 cudaStream_t st) {
   if (bdt == TCU_INT64)
-    return nz_run<VT, ACC, SPMV, long long>(vals, cols, x, x_len, static_cast<const long long*>(bounds), nseg, n, out,
-                                            ws, ws_bytes, st);
+    return bm_run<VT, ACC, CT, SPMV, long long>(vals, cols, x, x_len, static_cast<const long long*>(bounds), nb, n,
+                                                out, ws, ws_bytes, st);
   if (bdt == TCU_UINT32)
-    return nz_run<VT, ACC, SPMV, unsigned>(vals, cols, x, x_len, static_cast<const unsigned*>(bounds), nseg, n, out, ws,
-                                           ws_bytes, st);
-  return nz_run<VT, ACC, SPMV, int>(vals, cols, x, x_len, static_cast<const int*>(bounds), nseg, n, out, ws, ws_bytes,
-                                    st);
+    return bm_run<VT, ACC, CT, SPMV, unsigned>(vals, cols, x, x_len, static_cast<const unsigned*>(bounds), nb, n, out,
+                                               ws, ws_bytes, st);
+  return bm_run<VT, ACC, CT, SPMV, int>(vals, cols, x, x_len, static_cast<const int*>(bounds), nb, n, out, ws,
+                                        ws_bytes, st);
 }
 
 static tcu_status_t check_bounds(const void* bounds, tcu_dtype_t bdt) {
@@ -461,8 +486,8 @@ using namespace tcu;
 extern "C" {
 
 size_t tcu_rows_workspace_bytes(int64_t n) {
-  const int64_t tiles = (n + kNzTile - 1) / kNzTile;
-  return 128 + nz_scratch_bytes(tiles) + 16;
+  const int64_t tiles = (n + kBmMinTile - 1) / kBmMinTile;
+  return 128 + bm_scratch_bytes(tiles) + 16;
 }
 
 tcu_status_t tcu_seg_sum_rows(const void* x, tcu_dtype_t x_dtype, int64_t n, const void* bounds,
@@ -473,18 +498,17 @@ tcu_status_t tcu_seg_sum_rows(const void* x, tcu_dtype_t x_dtype, int64_t n, con
   if (!bounds || !out || (n > 0 && !x)) return TCU_ERR_ARG;
   tcu_status_t s = check_bounds(bounds, bounds_dtype);
   if (s != TCU_OK) return s;
-  const int64_t nseg = nbounds - 1;
   cudaStream_t st = (cudaStream_t)stream;
   switch (x_dtype) {
     case TCU_INT8:
-      return nz_dispatch<int8_t, int, false>((const int8_t*)x, nullptr, nullptr, 0, bounds, bounds_dtype, nseg, n,
-                                             (int*)out, ws, ws_bytes, st);
+      return bm_dispatch<int8_t, int, int, false>((const int8_t*)x, nullptr, nullptr, 0, bounds, bounds_dtype, nbounds,
+                                                  n, (int*)out, ws, ws_bytes, st);
     case TCU_FLOAT16:
-      return nz_dispatch<__half, float, false>((const __half*)x, nullptr, nullptr, 0, bounds, bounds_dtype, nseg, n,
-                                               (float*)out, ws, ws_bytes, st);
+      return bm_dispatch<__half, float, double, false>((const __half*)x, nullptr, nullptr, 0, bounds, bounds_dtype,
+                                                       nbounds, n, (float*)out, ws, ws_bytes, st);
     case TCU_FLOAT32:
-      return nz_dispatch<float, float, false>((const float*)x, nullptr, nullptr, 0, bounds, bounds_dtype, nseg, n,
-                                              (float*)out, ws, ws_bytes, st);
+      return bm_dispatch<float, float, double, false>((const float*)x, nullptr, nullptr, 0, bounds, bounds_dtype,
+                                                      nbounds, n, (float*)out, ws, ws_bytes, st);
     default:
       return TCU_ERR_DTYPE;
   }
@@ -500,11 +524,11 @@ tcu_status_t tcu_spmv_rows(const void* vals, tcu_dtype_t dtype, const void* indp
   if (s != TCU_OK) return s;
   cudaStream_t st = (cudaStream_t)stream;
   if (dtype == TCU_FLOAT16)
-    return nz_dispatch<__half, float, true>((const __half*)vals, cols, (const __half*)x, x_len, indptr, indptr_dtype,
-                                            rows, nnz, y, ws, ws_bytes, st);
+    return bm_dispatch<__half, float, double, true>((const __half*)vals, cols, (const __half*)x, x_len, indptr,
+                                                    indptr_dtype, rows + 1, nnz, y, ws, ws_bytes, st);
   if (dtype == TCU_FLOAT32)
-    return nz_dispatch<float, float, true>((const float*)vals, cols, (const float*)x, x_len, indptr, indptr_dtype,
-                                           rows, nnz, y, ws, ws_bytes, st);
+    return bm_dispatch<float, float, double, true>((const float*)vals, cols, (const float*)x, x_len, indptr,
+                                                   indptr_dtype, rows + 1, nnz, y, ws, ws_bytes, st);
   return TCU_ERR_DTYPE;
 }
 
