@@ -279,6 +279,29 @@ def measure_extras(dev, steps=10, warmup=3):
     out["seg_scan_flags_f16_2e28"] = entry(n, n * (2 + 1 + 4), ms, max_rel_err_vs_fp64=err)
     del xf, fl, zf, cs, sid, starts, base, ref
 
+    # per-segment sums (run_seg_sum_multi_core), fp16 2^28, int64 CSR-style
+    # bounds with geometric segment lengths of mean 64 and mean 4
+    xs16 = workloads.scan_input(n, torch.float16, dev, seed=14)
+    cs = torch.cumsum(xs16.double(), 0)
+    for mean in (64, 4):
+        g = torch.Generator(device=dev).manual_seed(15 + mean)
+        stp = torch.empty(n // mean + 4096, device=dev).geometric_(1.0 / mean, generator=g).to(torch.int64)
+        pts = torch.cumsum(stp, 0)
+        bnd = torch.cat([torch.zeros(1, dtype=torch.int64, device=dev), pts[pts < n],
+                         torch.full((1,), n, dtype=torch.int64, device=dev)])
+        del stp, pts
+        ms = _device_ms(lambda: tcuscan_ops.run_seg_sum_multi_core(xs16, bnd, 64), steps, warmup)
+        ys = tcuscan_ops.run_seg_sum_multi_core(xs16, bnd, 64)
+        hi = cs[bnd[1:] - 1]
+        lo = torch.where(bnd[:-1] > 0, cs[(bnd[:-1] - 1).clamp_min(0)], torch.zeros_like(hi))
+        refs = hi - lo
+        err = ((ys.double() - refs).abs() / refs.abs().clamp_min(1.0)).max().item()
+        nseg = bnd.numel() - 1
+        out[f"seg_sum_f16_2e28_mean{mean}"] = entry(n, n * 2 + (nseg + 1) * 8 + nseg * 4, ms, segments=nseg,
+                                                    max_rel_err_vs_fp64=err)
+        del bnd, ys, hi, lo, refs
+    del xs16, cs
+
     # CSR SpMV (products + indptr segment sums)
     for name, dt in (("spmv_f32", torch.float32), ("spmv_f16", torch.float16)):
         vals, indptr, cols, xs = workloads.zipf_csr(dtype=dt, device=dev, seed=9)
@@ -545,7 +568,8 @@ def _sig(v, digits=4):
     return v
 
 
-LEG_KEYS = ("scan_f16_2e28", "compress_f16", "compress_f32", "seg_scan_flags_f16_2e28", "spmv_f32", "spmv_f16",
+LEG_KEYS = ("scan_f16_2e28", "compress_f16", "compress_f32", "seg_scan_flags_f16_2e28", "seg_sum_f16_2e28_mean64",
+            "seg_sum_f16_2e28_mean4", "spmv_f32", "spmv_f16",
             "batch_rows_f32_4096", "scan_f16_2e20", "block_scan_f16_2e26_tensor_only", "block_scan_f16_2e26_engine")
 
 

@@ -96,6 +96,16 @@ TCU_API int tcu_get_max_ctas(void);
  * count; 0 disables the small tiles.  Process-wide. */
 TCU_API void tcu_set_small_tile_limit(int tiles);
 TCU_API int tcu_get_small_tile_limit(void);
+/* Tuning: full scans of at most `n` elements run in one SIMT pass -- 32
+ * input bytes per thread, a block scan, a one-warp look-back -- instead of
+ * on the tensor cores, whose per-tile chain of steps bounds small launches.
+ * Default (a negative value; tcu_get_simt_scan_limit then returns -1): 2^18
+ * fp16 / fp32 elements, 2^20 int8; 0 = never.  Same results up to FP32
+ * rounding inside a tile (exact for int8).  Process-wide; no reference
+ * counterpart (a launch-size choice inside run_scan_single_core /
+ * run_scan_multi_core, src/torch/torch_scan.h:47-110, 184-241). */
+TCU_API void tcu_set_simt_scan_limit(int64_t n);
+TCU_API int64_t tcu_get_simt_scan_limit(void);
 TCU_API tcu_status_t tcu_workspace_phase_ns(void* ws, uint64_t out[8], int clear, void* stream);
 
 /* ---- scans ---------------------------------------------------------------

@@ -240,12 +240,33 @@ static bool use_small_tiles(int64_t n) {
   return (n + 32767) / 32768 < lim;
 }
 
+// Full scans of at most this many elements run on the SIMT cores
+// (scan_small, tcu_scan_small.cu): below it the tensor-core tile chain, not
+// HBM, bounds the launch.  Measured on B200 (CUDA-graph replays): SIMT
+// ahead up to 2^18 fp16 / fp32 elements (6.3 vs 8.3 us at 2^14) and 2^20
+// int8 (8.3 vs 10.3 us), the tensor cores ahead from there (fp16 2^20: 10.3
+// vs 11.7 us).  tcu_set_simt_scan_limit sets one limit for every dtype
+// (0 = never, negative = these defaults).
+static int64_t g_simt_scan_limit = -1;
+static int64_t simt_limit(tcu_dtype_t dt) {
+  if (g_simt_scan_limit >= 0) return g_simt_scan_limit;
+  return dt == TCU_INT8 ? (int64_t(1) << 20) : (int64_t(1) << 18);
+}
+
+static bool valid_scan_S(tcu_dtype_t dt, int S) {
+  if (dt == TCU_INT8) return S == 32 || S == 64 || S == 128;
+  if (dt == TCU_FLOAT16) return S == 16 || S == 32 || S == 64 || S == 128;
+  return dt == TCU_FLOAT32;
+}
+
 template <int MODE>
 static tcu_status_t dispatch_scan(const void* x, tcu_dtype_t dt, int64_t n, int S, void* z, double start, int seg_rows,
                                   void* ws, size_t ws_bytes, cudaStream_t st, const void* start_dev = nullptr,
                                   int sk = -1) {
   if (sk < 0) sk = dt == TCU_INT8 ? 0 : 1;  // default device start: an output element (int32 / fp32)
   if constexpr (MODE == kScanFull) {
+    if (n <= simt_limit(dt) && valid_scan_S(dt, S))
+      return scan_small(x, dt, n, z, start, ws, ws_bytes, st, start_dev, sk);
     if (use_small_tiles(n))
       return dispatch_scan<kScanFullSmall>(x, dt, n, S, z, start, seg_rows, ws, ws_bytes, st, start_dev, sk);
   }
@@ -322,6 +343,8 @@ const char* tcu_last_error_message(void) { return g_errmsg; }
 void tcu_set_phase_profile(int enable) { g_phase_profile = enable ? 1 : 0; }
 void tcu_set_max_ctas(int n) { g_max_ctas = n > 0 ? n : 0; }
 void tcu_set_small_tile_limit(int tiles) { g_small_tile_limit = tiles < 0 ? -1 : tiles; }
+void tcu_set_simt_scan_limit(int64_t n) { g_simt_scan_limit = n < 0 ? -1 : n; }
+int64_t tcu_get_simt_scan_limit(void) { return g_simt_scan_limit; }
 int tcu_get_small_tile_limit(void) { return g_small_tile_limit < 0 ? sm_count() : g_small_tile_limit; }
 int tcu_get_max_ctas(void) { return g_max_ctas; }
 

@@ -21,6 +21,10 @@ TileDesc* ws_descs(void* ws);
 unsigned long long* ws_phase_counters(void* ws);
 // SpMV products written as pre-split fp32 rows (64 bf16 hi then 64 bf16 lo
 // per 64 products); prod holds roundup(nnz, 64) * 4 bytes.
+// Full scan on the SIMT cores for small inputs (tcu_scan_small.cu); start
+// plus the optional device start value as in the tensor-core scan.
+tcu_status_t scan_small(const void* x, tcu_dtype_t dt, int64_t n, void* z, double start, void* ws, size_t ws_bytes,
+                        cudaStream_t st, const void* start_dev, int start_dev_kind);
 tcu_status_t spmv_products_split(const void* values, tcu_dtype_t dtype, const int32_t* cols, int64_t nnz,
                                  const void* x, int64_t x_len, void* prod, void* ws, void* stream);
 

@@ -665,17 +665,19 @@ def _bounds_input(indptr, device, where):
 
 
 # Mean segment length up to which segment sums and SpMV take the element-split
-# SIMT kernels (tcu_seg_sum_rows / tcu_spmv_rows) instead of the tensor-core
-# segmented sum, which is bound by segment starts when segments are short.
-# Measured on B200 at 2^26 / 2^28 fp16 (CUDA-graph replays): the split path
-# is 3.7x faster at mean 4 and 1.2x at mean 16; the tensor cores are ahead
-# from mean 64 (0.14 vs 0.16 ms at 2^26).  SpMV on 2^20 Zipf(1.6) rows
-# (mean 16): 0.125 vs 0.228 ms.
-ROWS_MAX_MEAN = int(os.environ.get("TCU_ROWS_MAX_MEAN", "32"))
+# SIMT kernels (tcu_seg_sum_rows / tcu_spmv_rows: per-tile start/end bitmaps)
+# instead of the tensor-core segmented sum; 0 = every length, a negative
+# value = none (the tensor-core path for every length).  Measured on
+# B200 at 2^28 fp16 (geometric segment lengths): the bitmap path takes 0.71 /
+# 0.25 / 0.20 ms at mean 4 / 64 / 1024, the tensor-core path 0.48 / 0.36 ms
+# at mean 64 / 1024, so the split path serves every length by default.
+ROWS_MAX_MEAN = int(os.environ.get("TCU_ROWS_MAX_MEAN", "0"))
 
 
 def _use_rows(n, nseg):
-    return nseg > 0 and n <= ROWS_MAX_MEAN * nseg
+    if nseg <= 0 or ROWS_MAX_MEAN < 0:
+        return False
+    return ROWS_MAX_MEAN == 0 or n <= ROWS_MAX_MEAN * nseg
 
 
 # float32 segment sums (and SpMV, whose products are float32) always take

@@ -68,6 +68,8 @@ _sig("tcu_selftest_wait_timeout", _ST, _I, _U64, _P, _SZ, _P)
 _sig("tcu_get_max_ctas", _I)
 _sig("tcu_set_small_tile_limit", None, _I)
 _sig("tcu_get_small_tile_limit", _I)
+_sig("tcu_set_simt_scan_limit", None, _I64)
+_sig("tcu_get_simt_scan_limit", _I64)
 _sig("tcu_workspace_phase_ns", _ST, _P, ctypes.POINTER(ctypes.c_uint64), _I, _P)
 _sig("tcu_scan", _ST, _P, _I, _I64, _I, _D, _P, _P, _SZ, _P)
 _sig("tcu_scan_cpu", _ST, _P, _I, _I64, _P, _I)
@@ -124,8 +126,22 @@ def check(status, where):
         raise TcuError(status, where)
 
 
+_raw_stream_fn = getattr(torch._C, "_cuda_getCurrentRawStream", None)
+
+
+def _stream_key(dev):
+    """(device index, cudaStream_t as an int) of the current stream of
+    torch.device `dev` (the raw accessor skips building a torch.cuda.Stream
+    object: ~2 us per call of the small scans)."""
+    idx = dev.index if dev.index is not None else torch.cuda.current_device()
+    if _raw_stream_fn is not None:
+        return idx, _raw_stream_fn(idx)
+    return idx, torch.cuda.current_stream(torch.device("cuda", idx)).cuda_stream
+
+
 def stream_ptr(device):
-    return ctypes.c_void_p(torch.cuda.current_stream(device).cuda_stream)
+    dev = device if isinstance(device, torch.device) else torch.device(device)
+    return ctypes.c_void_p(_stream_key(dev)[1])
 
 
 class _Workspace:
@@ -158,8 +174,8 @@ def launch_context(device, need_bytes):
     stream): one current-stream lookup for both (the per-call host cost of
     the small scans is a few microseconds)."""
     dev = device if isinstance(device, torch.device) else torch.device(device)
-    stream = torch.cuda.current_stream(dev)
-    key = (dev.index, stream.cuda_stream)
+    key = _stream_key(dev)
+    sid = key[1]
     with _ws_lock:
         ws = _workspaces.get(key)
         if ws is None:
@@ -169,10 +185,10 @@ def launch_context(device, need_bytes):
             ws.buf = torch.empty(nbytes, dtype=torch.uint8, device=dev)
             ws.bytes = nbytes
             ws.ptr = None
-            check(lib.tcu_workspace_init(ctypes.c_void_p(ws.buf.data_ptr()), _SZ(nbytes),
-                                         ctypes.c_void_p(stream.cuda_stream)), "tcu_workspace_init")
+            check(lib.tcu_workspace_init(ctypes.c_void_p(ws.buf.data_ptr()), _SZ(nbytes), ctypes.c_void_p(sid)),
+                  "tcu_workspace_init")
         if ws.ptr is None:
-            ws.ptr = (ctypes.c_void_p(ws.buf.data_ptr()), _SZ(ws.bytes), ctypes.c_void_p(stream.cuda_stream))
+            ws.ptr = (ctypes.c_void_p(ws.buf.data_ptr()), _SZ(ws.bytes), ctypes.c_void_p(sid))
         return ws.ptr
 
 

@@ -114,3 +114,9 @@ def test_segment_sum_dispatch_rule(monkeypatch):
     assert not tcuscan_ops._rows_for(torch.float16, 10, 0)  # no segments
     monkeypatch.setattr(tcuscan_ops, "ROWS_FP32", False)
     assert not tcuscan_ops._rows_for(torch.float32, 1 << 20, 16)
+    monkeypatch.setattr(tcuscan_ops, "ROWS_MAX_MEAN", 0)  # 0: every length element-split (the default)
+    assert tcuscan_ops._rows_for(torch.float16, 1 << 20, 16)
+    assert tcuscan_ops._rows_for(torch.int8, 1 << 20, 1)
+    assert not tcuscan_ops._rows_for(torch.float16, 10, 0)
+    monkeypatch.setattr(tcuscan_ops, "ROWS_MAX_MEAN", -1)  # negative: the tensor-core path for every length
+    assert not tcuscan_ops._rows_for(torch.float16, 4 * 100, 100)

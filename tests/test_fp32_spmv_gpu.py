@@ -37,9 +37,21 @@ def _elementwise(got, ref):
     return float(np.max(np.abs(got - ref) / np.maximum(np.abs(ref), 1.0)))
 
 
+@pytest.fixture(params=["simt", "tensor"])
+def scan_path(request):
+    """Small full scans run on the SIMT cores; "tensor" sets the SIMT limit
+    to 0 so the same sizes run on the tensor cores."""
+    from tcuscan_ops import _lib
+
+    if request.param == "tensor":
+        _lib.lib.tcu_set_simt_scan_limit(0)
+    yield request.param
+    _lib.lib.tcu_set_simt_scan_limit(-1)
+
+
 @pytest.mark.parametrize("n", [1, 63, 64, 65, 8191, 8192 * 4 + 17, 1_000_003, 5_000_000])
 @pytest.mark.parametrize("start", [0.0, 7.5])
-def test_scan_single_core_fp32(n, start):
+def test_scan_single_core_fp32(n, start, scan_path):
     import tcuscan_ops
 
     g = torch.Generator().manual_seed(n)

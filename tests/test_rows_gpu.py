@@ -25,7 +25,7 @@ DEV = "cuda:0"
 def path(request, monkeypatch):
     import tcuscan_ops
 
-    monkeypatch.setattr(tcuscan_ops, "ROWS_MAX_MEAN", 1 << 40 if request.param == "rows" else 0)
+    monkeypatch.setattr(tcuscan_ops, "ROWS_MAX_MEAN", 1 << 40 if request.param == "rows" else -1)
     monkeypatch.setattr(tcuscan_ops, "ROWS_FP32", request.param == "rows")
     return request.param
 

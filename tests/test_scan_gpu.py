@@ -46,9 +46,22 @@ SIZES = [1, 2, 15, 16, 17, 127, 1000, 4095, 4096, 4097, 8191, 8192, 8193, 20 * 6
          20 * 64 * 64 + 129, 3 * 20 * 128 * 128 + 7, 1_000_003]
 
 
+@pytest.fixture(params=["simt", "tensor"])
+def scan_path(request):
+    """Full scans up to tcu_get_simt_scan_limit() elements run on the SIMT
+    cores; "tensor" sets the limit to 0 so the same sizes run on the tensor
+    cores (small tiles)."""
+    from tcuscan_ops import _lib
+
+    if request.param == "tensor":
+        _lib.lib.tcu_set_simt_scan_limit(0)
+    yield request.param
+    _lib.lib.tcu_set_simt_scan_limit(-1)
+
+
 @pytest.mark.parametrize("S", [32, 64, 128])
 @pytest.mark.parametrize("n", SIZES)
-def test_scan_int8(S, n):
+def test_scan_int8(S, n, scan_path):
     import tcuscan_ops
 
     x = _x(n, torch.int8, seed=n)
@@ -58,7 +71,7 @@ def test_scan_int8(S, n):
 
 @pytest.mark.parametrize("S", [16, 32, 64, 128])
 @pytest.mark.parametrize("n", SIZES)
-def test_scan_fp16(S, n):
+def test_scan_fp16(S, n, scan_path):
     import tcuscan_ops
 
     x = _x(n, torch.float16, seed=n)
@@ -67,7 +80,7 @@ def test_scan_fp16(S, n):
 
 
 @pytest.mark.parametrize("dtype", [torch.int8, torch.float16])
-def test_scan_2e20_config(dtype):
+def test_scan_2e20_config(dtype, scan_path):
     """The 1-D fp16 prefix sum config (n = 2^20, uniform[-1,1), S=64) and its int8 twin."""
     import tcuscan_ops
 
@@ -77,7 +90,7 @@ def test_scan_2e20_config(dtype):
 
 
 @pytest.mark.parametrize("dtype", [torch.int8, torch.float16])
-def test_scan_single_core_starting_sum(dtype):
+def test_scan_single_core_starting_sum(dtype, scan_path):
     import tcuscan_ops
 
     for n, start in ((100, 7), (64 * 64 * 3 - 17, -11), (200_001, 5)):
