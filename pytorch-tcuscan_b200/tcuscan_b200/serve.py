@@ -14,14 +14,19 @@ its stream.  This module keeps the device busy with many requests at once:
   inputs, outputs, row pointers and the batch's request table.  Requests keep
   arriving while earlier batches run; the next batch takes whatever has
   arrived (continuous batching), oldest class first.
-- A batch is one pack launch (``tcu_pack``: every request's elements copied
-  back to back into the block, each request on a 256-element boundary,
-  padding zeroed; seg_sum row pointers rebased by the request's offset) and
-  one segmented launch over the packed buffer: ``tcu_seg_bounds`` with the
-  request starts as segment starts (scan), with the rebased row pointers and
-  per-segment sums (seg_sum), or ``tcu_compress_segments`` (compress, with
-  each request's output offset).  Batches on different slots run on
-  different CUDA streams and overlap on the GPU.
+- Scan and seg_sum requests of ``SOLO_MIN`` (2^20) elements or more are
+  read in place: each runs the single-call kernel (``tcu_scan`` /
+  ``tcu_seg_sum_rows`` on its own values and row pointers) into its batch's
+  block, so the bulk of the served bytes is never copied.  The smaller
+  requests of a batch take one pack launch (``tcu_pack``: every request's
+  elements copied back to back into the block, each request on a
+  256-element boundary, padding zeroed; seg_sum row pointers rebased by the
+  request's offset) and one segmented launch over the packed buffer:
+  ``tcu_seg_bounds`` with the request starts as segment starts (scan), the
+  element-split segment sums over the rebased row pointers (seg_sum), or
+  ``tcu_compress_segments`` (compress -- every compress request is packed,
+  with its output offset).  Batches on different slots run on different
+  CUDA streams and overlap on the GPU.
 - Completion is read from one CUDA event per slot (polled, never a device
   synchronisation).  A request's result is a view of its batch's block.
 
@@ -46,6 +51,10 @@ DTYPES = (torch.int8, torch.float16, torch.float32)
 _DT_INDEX = {d: i for i, d in enumerate(DTYPES)}
 _EB = np.array([1, 2, 4], dtype=np.int64)
 ALIGN = 256        # elements: every request starts on a 256-element boundary of its batch
+# scan / seg_sum requests of at least this many elements are not packed: each
+# runs the single-call kernel on its own input in place (the pack copy would
+# read and write every input byte once more), writing into its batch's block
+SOLO_MIN = 1 << 20
 BLOCK_ALIGN = 256  # bytes: arena blocks and the buffers inside them
 BATCH_SLACK = 8192  # bytes per batch for buffer alignment inside its block
 
@@ -393,32 +402,42 @@ class Server:
             raise MemoryError("arena allocation failed")
         self.used += nbytes
         self.peak_used = max(self.peak_used, self.used)
-        n = self.n[ids]
-        k = ids.size
+        self.admit[ids] = self.now()
+        # requests read in place (large scan / seg_sum inputs, 16-byte aligned)
+        # and the rest, which are packed back to back
+        solo = np.zeros(ids.size, dtype=bool)
+        if op in (SCAN, SEG_SUM):
+            solo = (self.n[ids] >= SOLO_MIN) & (self.xp[ids] % 16 == 0)
+            if op == SEG_SUM:
+                solo &= self.ap[ids] % 8 == 0
+        ids_p, ids_s = ids[~solo], ids[solo]
+        n = self.n[ids_p]
+        k = ids_p.size
         npad = _roundup(n, ALIGN)
         dst = np.zeros(k, dtype=np.int64)
-        np.cumsum(npad[:-1], out=dst[1:])
+        if k:
+            np.cumsum(npad[:-1], out=dst[1:])
         total = int(npad.sum())
-        self.admit[ids] = self.now()
 
-        # request table of the batch, staged in the slot's pinned buffer
+        # request table of the packed part, staged in the slot's pinned buffer
         items = np.empty(k, dtype=PACK_ITEM)
-        items["src"], items["dst"], items["n"], items["len"], items["add"] = self.xp[ids], dst, n, npad, 0
+        items["src"], items["dst"], items["n"], items["len"], items["add"] = self.xp[ids_p], dst, n, npad, 0
         meta = [items.view(np.uint8)]
         if op == SEG_SUM:
-            nb = self.nseg[ids] + 1
+            nb = self.nseg[ids_p] + 1
             boff = np.zeros(k, dtype=np.int64)
-            np.cumsum(nb[:-1], out=boff[1:])
+            if k:
+                np.cumsum(nb[:-1], out=boff[1:])
             bitems = np.empty(k, dtype=PACK_ITEM)
-            bitems["src"], bitems["dst"], bitems["n"], bitems["len"], bitems["add"] = self.ap[ids], boff, nb, nb, dst
+            bitems["src"], bitems["dst"], bitems["n"], bitems["len"], bitems["add"] = self.ap[ids_p], boff, nb, nb, dst
             meta.append(bitems.view(np.uint8))
         elif op == COMPRESS:
             mitems = items.copy()
-            mitems["src"] = self.ap[ids]
+            mitems["src"] = self.ap[ids_p]
             meta += [mitems.view(np.uint8), dst.view(np.uint8)]
         else:
             meta.append(dst.view(np.uint8))
-        mb = sum(m.size for m in meta)
+        mb = max(sum(m.size for m in meta), 16)
         if mb > sl.pinned.numel():
             sl.pinned = torch.empty(_roundup(mb, 1 << 20), dtype=torch.uint8, pin_memory=True)
         pn = sl.pinned.numpy()
@@ -441,36 +460,61 @@ class Server:
         ab = self.arena.buf
         st = sl.stream
         sp = ctypes.c_void_p(st.cuda_stream)
-        S = tcuscan_ops._pick_S(self.S, dtype, total, op="seg")
+        S = tcuscan_ops._pick_S(self.S, dtype, max(total, 1), op="seg")
         L = _lib.lib
+        wsp = sl.ws.data_ptr()
         with torch.cuda.stream(st):
-            ab[m_off:m_off + mb].copy_(sl.pinned[:mb], non_blocking=True)
-            tcuscan_ops.check(L.tcu_pack(base + m_off, k, eb, eb, base + x_off, total, sp), "serve pack")
+            if k:
+                ab[m_off:m_off + mb].copy_(sl.pinned[:mb], non_blocking=True)
+                tcuscan_ops.check(L.tcu_pack(base + m_off, k, eb, eb, base + x_off, total, sp), "serve pack")
             if op == SCAN:
                 out_dtype = tcuscan_ops._scan_out_dtype(dtype)
-                z_off = carve(total * 4)
-                s_ = L.tcu_seg_bounds(base + x_off, _lib.DTYPE_CODE[dtype], total, S, base + m_off + items.nbytes,
-                                      _lib.TCU_INT64, k, 0, base + z_off, sl.ws.data_ptr(), sl.wsb, sp)
-                tcuscan_ops.check(s_, "serve scan")
-                self.roff[ids], self.rlen[ids] = dst, n
-                out_len = total
+                npad_s = _roundup(self.n[ids_s], ALIGN)
+                z_off = carve((total + int(npad_s.sum())) * 4)
+                if k:
+                    s_ = L.tcu_seg_bounds(base + x_off, _lib.DTYPE_CODE[dtype], total, S, base + m_off + items.nbytes,
+                                          _lib.TCU_INT64, k, 0, base + z_off, wsp, sl.wsb, sp)
+                    tcuscan_ops.check(s_, "serve scan")
+                    self.roff[ids_p], self.rlen[ids_p] = dst, n
+                o_ = total
+                for j, r in enumerate(ids_s):  # in place: the single call's scan
+                    nr = int(self.n[r])
+                    S_r = tcuscan_ops._pick_S(self.S, dtype, nr)
+                    s_ = L.tcu_scan(int(self.xp[r]), _lib.DTYPE_CODE[dtype], nr, S_r, 0.0, base + z_off + o_ * 4,
+                                    wsp, sl.wsb, sp)
+                    tcuscan_ops.check(s_, "serve scan (in place)")
+                    self.roff[r], self.rlen[r] = o_, nr
+                    o_ += int(npad_s[j])
+                out_len = max(o_, 1)
             elif op == SEG_SUM:
                 out_dtype = tcuscan_ops._scan_out_dtype(dtype)
-                nbt = int(nb.sum())
-                b_off = carve(nbt * 8)
-                z_off = carve(max(nbt - 1, 1) * 4)
                 iw = int(self.iw[ids[0]])
-                tcuscan_ops.check(L.tcu_pack(base + m_off + items.nbytes, k, iw, 8, base + b_off, nbt, sp),
-                                  "serve pack row pointers")
-                if tcuscan_ops._rows_for(dtype, total, nbt - 1):  # same rule as run_seg_sum_*
-                    s_ = L.tcu_seg_sum_rows(base + x_off, _lib.DTYPE_CODE[dtype], total, base + b_off,
-                                            _lib.TCU_INT64, nbt, base + z_off, sl.ws.data_ptr(), sl.wsb, sp)
-                else:
-                    s_ = L.tcu_seg_bounds(base + x_off, _lib.DTYPE_CODE[dtype], total, S, base + b_off,
-                                          _lib.TCU_INT64, nbt, 1, base + z_off, sl.ws.data_ptr(), sl.wsb, sp)
-                tcuscan_ops.check(s_, "serve seg_sum")
-                self.roff[ids], self.rlen[ids] = boff, self.nseg[ids]
-                out_len = max(nbt - 1, 1)
+                nbt = int(nb.sum()) if k else 0
+                b_off = carve(nbt * 8)
+                out_p = max(nbt - 1, 0)
+                z_off = carve(max(out_p + int(self.nseg[ids_s].sum()), 1) * 4)
+                if k:
+                    tcuscan_ops.check(L.tcu_pack(base + m_off + items.nbytes, k, iw, 8, base + b_off, nbt, sp),
+                                      "serve pack row pointers")
+                    if tcuscan_ops._rows_for(dtype, total, nbt - 1):  # same rule as run_seg_sum_*
+                        s_ = L.tcu_seg_sum_rows(base + x_off, _lib.DTYPE_CODE[dtype], total, base + b_off,
+                                                _lib.TCU_INT64, nbt, base + z_off, wsp, sl.wsb, sp)
+                    else:
+                        s_ = L.tcu_seg_bounds(base + x_off, _lib.DTYPE_CODE[dtype], total, S, base + b_off,
+                                              _lib.TCU_INT64, nbt, 1, base + z_off, wsp, sl.wsb, sp)
+                    tcuscan_ops.check(s_, "serve seg_sum")
+                    self.roff[ids_p], self.rlen[ids_p] = boff, self.nseg[ids_p]
+                o_ = out_p
+                bdt = _lib.TCU_INT64 if iw == 8 else _lib.TCU_INT32
+                for r in ids_s:  # in place: the request's own values and row pointers
+                    nr, ns = int(self.n[r]), int(self.nseg[r])
+                    if ns > 0:
+                        s_ = L.tcu_seg_sum_rows(int(self.xp[r]), _lib.DTYPE_CODE[dtype], nr, int(self.ap[r]), bdt,
+                                                ns + 1, base + z_off + o_ * 4, wsp, sl.wsb, sp)
+                        tcuscan_ops.check(s_, "serve seg_sum (in place)")
+                    self.roff[r], self.rlen[r] = o_, ns
+                    o_ += ns
+                out_len = max(o_, 1)
             else:
                 out_dtype = dtype
                 mk_off = carve(total)
@@ -480,7 +524,7 @@ class Server:
                                   "serve pack masks")
                 starts = base + m_off + 2 * items.nbytes
                 s_ = L.tcu_compress_segments(base + x_off, eb, base + mk_off, total, starts, k, base + z_off, total,
-                                             base + p_off, sl.ws.data_ptr(), sl.wsb, sp)
+                                             base + p_off, wsp, sl.wsb, sp)
                 tcuscan_ops.check(s_, "serve compress")
                 sl.pos_host[: k + 1].copy_(ab[p_off:p_off + (k + 1) * 8].view(torch.int64), non_blocking=True)
                 out_len = total

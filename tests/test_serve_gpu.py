@@ -201,6 +201,44 @@ def test_server_mix_equals_alone_and_oracle():
     tcuscan_ops.raise_device_error(DEV)
 
 
+def test_server_in_place_requests(monkeypatch):
+    """Scan / seg_sum requests at or above SOLO_MIN run the single-call kernel
+    on their own inputs (no pack copy), beside packed requests of the same
+    batch: every result equals the oracle (integers bit for bit) and the
+    single drop-in call."""
+    import tcuscan_ops
+    from tcuscan_b200 import serve
+
+    monkeypatch.setattr(serve, "SOLO_MIN", 1 << 12)
+    reqs = _mixed_requests(48, 11, max_log2=15)
+    srv = serve.Server(DEV, budget_bytes=1 << 30, slots=2, max_batch=24, keep_results=True)
+    ids = [srv.submit(op, x, aux) for op, x, aux in reqs]
+    srv.run()
+    n_solo = sum(1 for op, x, _ in reqs if op != "compress" and x.numel() >= (1 << 12))
+    assert 0 < n_solo < len(reqs)
+    for rid, (op, x, aux) in zip(ids, reqs):
+        got = srv.result(rid).cpu()
+        exact = x.dtype == torch.int8 or op == "compress"
+        if op == "scan" and x.dtype == torch.int8:
+            ref = torch.cumsum(x.cpu().long(), 0).int().numpy()
+        else:
+            ref = _oracle(op, x, aux)
+        assert got.shape[0] == np.asarray(ref).shape[0], (rid, op)
+        assert _close(got.numpy(), ref, exact), (rid, op, x.dtype)
+        if op == "scan" and x.numel() >= (1 << 12):  # in place: the single call's own kernel
+            single = tcuscan_ops.run_scan_multi_core(x, tcuscan_ops._pick_S(None, x.dtype, x.numel())).cpu()
+            if exact:
+                assert torch.equal(got, single), rid
+            else:  # only the order of the FP64 tile carries may differ
+                d = (got.double() - single.double()).abs().max().item()
+                assert d <= TOL * max(1.0, single.double().abs().max().item()), rid
+        elif op == "seg_sum" and x.numel() >= (1 << 12):
+            single = tcuscan_ops.run_seg_sum_multi_core(x, aux, 64).cpu()
+            assert torch.equal(got, single), rid
+    srv.release()
+    tcuscan_ops.raise_device_error(DEV)
+
+
 def test_server_budget_admission_and_arrivals():
     from tcuscan_b200 import serve
 
