@@ -90,8 +90,39 @@ static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 
 // 2-D row-major tensor [rows, cols] of `elem`-byte elements, box [box_rows,
 // box_cols], swizzle span = box_cols * elem bytes (32/64/128; 16 = unswizzled).
+// The last few encoded maps of this thread, by their arguments: a repeated
+// call on the same buffers (the small scans of a serving loop or a chained
+// host scan) copies the map instead of encoding it again (~1 us each).
+namespace {
+struct MapKey {
+  const void* base;
+  uint64_t cols, rows;
+  int dt, elem;
+  uint32_t box_cols, box_rows;
+  bool operator==(const MapKey& o) const {
+    return base == o.base && cols == o.cols && rows == o.rows && dt == o.dt && elem == o.elem &&
+           box_cols == o.box_cols && box_rows == o.box_rows;
+  }
+};
+struct MapCache {
+  static constexpr int N = 8;
+  MapKey key[N];
+  CUtensorMap map[N];
+  bool used[N] = {};
+  int next = 0;
+};
+thread_local MapCache t_maps;
+}  // namespace
+
 tcu_status_t make_map_2d(CUtensorMap* m, const void* base, CUtensorMapDataType dt, int elem, uint64_t cols,
                          uint64_t rows, uint32_t box_cols, uint32_t box_rows) {
+  const MapKey k{base, cols, rows, (int)dt, elem, box_cols, box_rows};
+  for (int i = 0; i < MapCache::N; ++i) {
+    if (t_maps.used[i] && t_maps.key[i] == k) {
+      *m = t_maps.map[i];
+      return TCU_OK;
+    }
+  }
   auto fn = encode_fn();
   if (!fn) {
     snprintf(g_errmsg, sizeof(g_errmsg), "cuTensorMapEncodeTiled entry point unavailable");
@@ -112,6 +143,11 @@ tcu_status_t make_map_2d(CUtensorMap* m, const void* base, CUtensorMapDataType d
     snprintf(g_errmsg, sizeof(g_errmsg), "cuTensorMapEncodeTiled failed (%d)", (int)r);
     return TCU_ERR_LAUNCH;
   }
+  const int slot = t_maps.next;
+  t_maps.next = (slot + 1) % MapCache::N;
+  t_maps.key[slot] = k;
+  t_maps.map[slot] = *m;
+  t_maps.used[slot] = true;
   return TCU_OK;
 }
 
