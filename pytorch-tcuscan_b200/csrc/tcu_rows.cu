@@ -9,8 +9,8 @@
 // segment lengths:
 //   bm_tile_first_kernel  one warp per tile: the first bound at or after the
 //                         tile start (a 32-way search);
-//   bm_segsum_kernel      one CTA per tile, 128 bytes of input per thread
-//                         (32 elements for SpMV: it gathers x[cols] and
+//   bm_segsum_kernel      one CTA per tile, 64 bytes of input per thread
+//                         (32 elements for fp32 and for SpMV: it gathers x[cols] and
 //                         multiplies in FP32), loads issued first.  The
 //                         tile's bounds set two bitmaps in shared memory, one
 //                         bit per element: segment starts and segment ends
@@ -42,12 +42,17 @@ namespace tcu {
 
 constexpr int kBmThreads = 256;
 constexpr int kBmWarps = kBmThreads / 32;
-// Elements per thread: 128 bytes of input (32 for SpMV, whose products take
-// a register each), so a CTA moves 32 KB per tile.  The boundary bitmaps
-// give every element one bit: thread t owns words [t * IPT / 32, ...).
+// Elements per thread: 64 bytes of input (fp16 32, int8 64), 32 elements
+// for fp32 and SpMV (whose products take a register each).  Fewer bytes per
+// thread leave fewer registers per thread and more CTAs per SM, which hide
+// the per-tile chain of dependent loads better: 128 bytes per thread at 4
+// CTAs per SM measured 0.71 / 0.25 / 0.20 ms at mean segment 4 / 64 / 1024
+// (2^28 fp16), 64 bytes at up to 6 CTAs per SM 0.62 / 0.22 / 0.19 ms.  The
+// boundary bitmaps give every element one bit: thread t owns words
+// [t * IPT / 32, ...).
 template <typename VT, bool SPMV>
 struct BmCfg {
-  static constexpr int IPT = SPMV ? 32 : 128 / (int)sizeof(VT);
+  static constexpr int IPT = SPMV ? 32 : (64 / (int)sizeof(VT) < 32 ? 32 : 64 / (int)sizeof(VT));
   static constexpr int WPT = IPT / 32;  // bitmap words per thread
   static constexpr int TILE = kBmThreads * IPT;
 };
@@ -121,7 +126,7 @@ __device__ __forceinline__ int64_t bm_lower_bound(const IT* bounds, int64_t lo, 
 // int32 for int8); CT: cross-tile carry type; SPMV: element i is
 // vals[i] * x[cols[i]] (FP32 product), else vals[i].
 template <typename VT, typename ACC, typename CT, bool SPMV, typename IT>
-__global__ void __launch_bounds__(kBmThreads, SPMV ? 3 : 4) bm_segsum_kernel(const VT* __restrict__ vals,
+__global__ void __launch_bounds__(kBmThreads, SPMV ? 3 : (sizeof(VT) == 4 ? 4 : 6)) bm_segsum_kernel(const VT* __restrict__ vals,
                                                                   const int32_t* __restrict__ cols,
                                                                   const VT* __restrict__ x, int64_t x_len,
                                                                   const IT* __restrict__ bounds, int64_t nb,

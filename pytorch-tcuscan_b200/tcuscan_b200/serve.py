@@ -14,7 +14,7 @@ its stream.  This module keeps the device busy with many requests at once:
   inputs, outputs, row pointers and the batch's request table.  Requests keep
   arriving while earlier batches run; the next batch takes whatever has
   arrived (continuous batching), oldest class first.
-- Scan and seg_sum requests of ``SOLO_MIN`` (2^20) elements or more are
+- Scan and seg_sum requests of ``SOLO_MIN`` (2^22) elements or more are
   read in place: each runs the single-call kernel (``tcu_scan`` /
   ``tcu_seg_sum_rows`` on its own values and row pointers) into its batch's
   block, so the bulk of the served bytes is never copied.  The smaller
@@ -53,8 +53,12 @@ _EB = np.array([1, 2, 4], dtype=np.int64)
 ALIGN = 256        # elements: every request starts on a 256-element boundary of its batch
 # scan / seg_sum requests of at least this many elements are not packed: each
 # runs the single-call kernel on its own input in place (the pack copy would
-# read and write every input byte once more), writing into its batch's block
-SOLO_MIN = 1 << 20
+# read and write every input byte once more), writing into its batch's block.
+# Each one costs a launch from the host loop, so the threshold trades copied
+# bytes against launches: on the served stream (20000 requests, log-uniform
+# sizes in [2^10, 2^24]) everything packed gave 2.39 TB/s, 2^20 2.15, 2^21
+# 2.39, 2^22 2.54 and 2^23 2.55 TB/s.
+SOLO_MIN = 1 << 22
 BLOCK_ALIGN = 256  # bytes: arena blocks and the buffers inside them
 BATCH_SLACK = 8192  # bytes per batch for buffer alignment inside its block
 
