@@ -139,7 +139,7 @@ __global__ void __launch_bounds__(kBmThreads, SPMV ? 3 : (sizeof(VT) == 4 ? 4 : 
   __shared__ uint32_t sE[kBmThreads * WPT];  // segment-end bits (the last element of every non-empty segment)
   __shared__ ACC swv[kBmWarps];
   __shared__ int swf[kBmWarps], swc[kBmWarps];
-  __shared__ __align__(16) ACC sP[kBmThreads * 36];  // per-thread word prefixes (row of 36)
+  __shared__ __align__(16) ACC sP[kBmThreads * 32];  // per-thread word prefixes (row of 32, chunks swizzled)
   __shared__ unsigned long long s_kfirst;  // output index of the tile's first end
   __shared__ int s_empty;                  // the tile's bounds hold an empty segment
   const int t = threadIdx.x, lane = t & 31, w = t >> 5;
@@ -298,11 +298,15 @@ __global__ void __launch_bounds__(kBmThreads, SPMV ? 3 : (sizeof(VT) == 4 ? 4 : 
 
   // ---- the thread's segmented sums, a word (32 elements) at a time: the
   // word's inclusive prefix P goes to the thread's row of shared memory
-  // (36 entries: rows 144 bytes apart, so the 16-byte stores of 8 lanes hit
-  // distinct banks), then every end e takes P[e] - P[s - 1] for the last
+  // (32 entries; 16-byte chunk c of row t at c ^ (t & 7), so the 16-byte
+  // stores of 8 lanes hit distinct banks without padding the rows -- 32 KB
+  // per CTA instead of 36 KB, one more CTA per SM), then every end e takes
+  // P[e] - P[s - 1] for the last
   // start s <= e in the word, or P[e] plus the sum carried in from before
   // the word.  No per-element branch: the ends are visited by bit. ----
-  ACC* myP = sP + t * 36;
+  ACC* myP = sP + t * 32;
+  const int sx = t & 7;
+  auto pat = [&](int i) -> ACC { return myP[(((i >> 2) ^ sx) << 2) | (i & 3)]; };
   ACC running = ACC(0);  // sum since the thread's last start (everything so far without one)
   bool open = true;      // no start seen yet in this thread
   int open_ord = -1, open_e = 0;
@@ -326,7 +330,7 @@ __global__ void __launch_bounds__(kBmThreads, SPMV ? 3 : (sizeof(VT) == 4 ? 4 : 
           u.y = *reinterpret_cast<const uint32_t*>(&a1);
           u.z = *reinterpret_cast<const uint32_t*>(&a2);
           u.w = *reinterpret_cast<const uint32_t*>(&a3);
-          *reinterpret_cast<uint4*>(myP + 4 * i4) = u;
+          *reinterpret_cast<uint4*>(myP + 4 * (i4 ^ sx)) = u;
         }
       }
       pfx = a3;
@@ -335,11 +339,11 @@ __global__ void __launch_bounds__(kBmThreads, SPMV ? 3 : (sizeof(VT) == 4 ? 4 : 
       const int i = __ffs(em) - 1;
       em &= em - 1u;
       const uint32_t sb = sw & (0xFFFFFFFFu >> (31 - i));  // starts at or before i
-      const ACC pe = myP[i];
+      const ACC pe = pat(i);
       const int e = t * IPT + q * 32 + i;
       if (sb) {
         const int ls = 31 - __clz(sb);
-        out[out_index(ord, e)] = pe - (ls ? myP[ls - 1] : ACC(0));
+        out[out_index(ord, e)] = pe - (ls ? pat(ls - 1) : ACC(0));
       } else if (!open) {
         out[out_index(ord, e)] = running + pe;
       } else {  // the segment began before this thread: finished after the carry scan
@@ -351,7 +355,7 @@ __global__ void __launch_bounds__(kBmThreads, SPMV ? 3 : (sizeof(VT) == 4 ? 4 : 
     }
     if (sw) {
       const int ls = 31 - __clz(sw);
-      running = pfx - (ls ? myP[ls - 1] : ACC(0));
+      running = pfx - (ls ? pat(ls - 1) : ACC(0));
       open = false;
     } else {
       running += pfx;
