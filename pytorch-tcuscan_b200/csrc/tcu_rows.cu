@@ -214,6 +214,18 @@ __global__ void __launch_bounds__(kBmThreads, SPMV ? 3 : (sizeof(VT) == 4 ? 4 : 
     }
   }
 
+  // ---- SpMV: gather x[cols] (FP32 products), issued before the bounds
+  // work so their L2 latency overlaps the chain first bound index ->
+  // bounds -> bitmaps ----
+  if constexpr (SPMV) {
+#pragma unroll
+    for (int i = 0; i < IPT; ++i) {
+      float xv = 0.f;
+      if ((unsigned long long)(unsigned)cc[i] < (unsigned long long)x_len) xv = elem_f32<VT>(x + cc[i]);
+      else if (i < nvalid && ws) record_error(ws, TCU_ERR_ARG, 301, (uint32_t)(j0 + i));
+      pv[i] = __fmul_rn(pv[i], xv);
+    }
+  }
   // ---- boundary bitmaps from the tile's bounds ----
 #pragma unroll
   for (int q = 0; q < WPT; ++q) {
@@ -269,16 +281,6 @@ __global__ void __launch_bounds__(kBmThreads, SPMV ? 3 : (sizeof(VT) == 4 ? 4 : 
   for (int k = 0; k < kBmWarps; ++k) wpre += k < w ? swc[k] : 0;
   int ord = wpre + ecs - ec;
 
-  // ---- SpMV: gather x[cols] (FP32 products) ----
-  if constexpr (SPMV) {
-#pragma unroll
-    for (int i = 0; i < IPT; ++i) {
-      float xv = 0.f;
-      if ((unsigned long long)(unsigned)cc[i] < (unsigned long long)x_len) xv = elem_f32<VT>(x + cc[i]);
-      else if (i < nvalid && ws) record_error(ws, TCU_ERR_ARG, 301, (uint32_t)(j0 + i));
-      pv[i] = __fmul_rn(pv[i], xv);
-    }
-  }
   auto elem = [&](int i) -> ACC {
     if constexpr (SPMV) {
       return pv[i];
