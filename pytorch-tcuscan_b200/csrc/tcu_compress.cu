@@ -74,12 +74,21 @@ struct ElemT<8> { using T = unsigned long long; };
 // Elements per worker row for an element / index size: at most 128 bytes of
 // payload per array and row; a tile is 128 rows.
 __host__ __device__ constexpr int cmp_ept(int eb, int ib) { return eb + ib <= 2 ? 64 : (eb + ib <= 4 ? 32 : 16); }
+// Elements per row for an index mode: gathered indices (1) are staged like
+// the values; generated positions (2) need only a 16-bit tile-local offset
+// per element in the compaction scratch, so they keep the values' row length
+// (fp16 / int8: 64, as without indices) wherever the stage ring still holds
+// five stages.  Staging 4-byte positions instead cut fp16 rows to 16
+// elements and took 620 us at 2^28 against 205 us without positions.
+__host__ __device__ constexpr int cmp_ept_for(int eb, int idx_mode, int ib) {
+  return idx_mode == 2 ? (eb <= 2 ? 64 : (eb == 4 ? 32 : 16)) : cmp_ept(eb, idx_mode ? ib : 0);
+}
 
 template <int EB, int IDX, int IB>
 struct CmpCfg {
-  static constexpr int IBX = IDX ? IB : 0;     // index bytes held in the stage
+  static constexpr int IBX = IDX == 1 ? IB : (IDX == 2 ? 2 : 0);  // index bytes per element in the stage
   static constexpr int RB = EB + IBX;
-  static constexpr int EPT = cmp_ept(EB, IBX);
+  static constexpr int EPT = cmp_ept_for(EB, IDX, IB);
   static constexpr int TILE = 128 * EPT;
   static constexpr int SPAN_M = EPT;           // bytes of one mask row
   static constexpr int SPAN_X = EPT * EB;      // bytes of one value row
@@ -92,8 +101,9 @@ struct CmpCfg {
   static constexpr int CTRL = 1024;
   static constexpr int SMEM = CTRL + NST * STAGE + 1024;  // + alignment slack
   static_assert(NST >= kCmpWG + 1, "stage ring too short");
-  static_assert(SPAN_X <= 128 && SPAN_M <= 128 && (IDX == 0 || SPAN_I <= 128), "row span");
+  static_assert(SPAN_X <= 128 && SPAN_M <= 128 && (IDX != 1 || SPAN_I <= 128), "row span");
   static_assert(STAGE % 1024 == 0, "stage alignment");
+  static_assert(IDX != 2 || TILE <= 65536, "tile-local positions are 16-bit");
 };
 
 struct CmpCtrl {
@@ -312,6 +322,8 @@ __global__ void __launch_bounds__(kCmpThreads, 1)
       {
         T* sx = reinterpret_cast<T*>(st + C::X_OFF);
         I* si = reinterpret_cast<I*>(st + C::I_OFF);
+        uint16_t* sp = reinterpret_cast<uint16_t*>(st + C::I_OFF);  // IDX 2: tile-local positions
+        const int lrow = wg_thread * EPT;                           // this row's first position in the tile
         int o = local;
         if constexpr (SPLIT) {
           // unselected elements before this row: all earlier rows of the tile are full
@@ -324,7 +336,7 @@ __global__ void __launch_bounds__(kCmpThreads, 1)
               const int d = on ? o : u;
               sx[d] = vec_elem<EB>(xr, j);
               if constexpr (IDX == 1) si[d] = (I)vec_elem<(IB > 0 ? IB : 4)>(ir, j);
-              if constexpr (IDX == 2) si[d] = (I)(e0 + j);
+              if constexpr (IDX == 2) sp[d] = (uint16_t)(lrow + j);
               o += on ? 1 : 0;
               u += on ? 0 : 1;
             }
@@ -335,7 +347,7 @@ __global__ void __launch_bounds__(kCmpThreads, 1)
             if ((sel >> j) & 1ull) {
               sx[o] = vec_elem<EB>(xr, j);
               if constexpr (IDX == 1) si[o] = (I)vec_elem<(IB > 0 ? IB : 4)>(ir, j);
-              if constexpr (IDX == 2) si[o] = (I)(e0 + j);
+              if constexpr (IDX == 2) sp[o] = (uint16_t)(lrow + j);
               ++o;
             }
           }
@@ -347,6 +359,7 @@ __global__ void __launch_bounds__(kCmpThreads, 1)
       {
         const T* sx = reinterpret_cast<const T*>(st + C::X_OFF);
         const I* si = reinterpret_cast<const I*>(st + C::I_OFF);
+        const uint16_t* sp = reinterpret_cast<const uint16_t*>(st + C::I_OFF);
         const int64_t t0 = (int64_t)tid * TILE;
         const int valid = SPLIT ? (int)(p.n - t0 < TILE ? p.n - t0 : TILE) : total;
         // selected run at pre, unselected run after every selected element
@@ -355,7 +368,8 @@ __global__ void __launch_bounds__(kCmpThreads, 1)
           const long long g = i < total ? pre + i : ubase + i;
           if (g < p.capacity) {
             static_cast<T*>(p.out)[g] = sx[i];
-            if constexpr (IDX != 0) static_cast<I*>(p.idx_out)[g] = si[i];
+            if constexpr (IDX == 1) static_cast<I*>(p.idx_out)[g] = si[i];
+            if constexpr (IDX == 2) static_cast<I*>(p.idx_out)[g] = (I)(t0 + sp[i]);
           }
         }
       }
@@ -513,9 +527,9 @@ __global__ void __launch_bounds__(256) mask_count_kernel(const int8_t* mask, int
 // per-tile counts and offsets sit in the workspace's descriptor region:
 // offsets[num_tiles + 1] (int64), counts[num_tiles] (int32), then one int64
 // block total per 1024 tiles.
-static int64_t compress_tile(int elem_bytes, int idx_bytes) { return 128 * cmp_ept(elem_bytes, idx_bytes); }
-
-static int idx_stage_bytes(int idx_mode, int idx_bytes) { return idx_mode ? idx_bytes : 0; }
+static int64_t compress_tile(int elem_bytes, int idx_mode, int idx_bytes) {
+  return 128 * cmp_ept_for(elem_bytes, idx_mode, idx_bytes);
+}
 
 struct CmpScratch {
   long long* offsets;
@@ -693,7 +707,7 @@ tcu_status_t tcu_compress_count(const int8_t* mask, int64_t n, int elem_bytes, i
   if (!mask) return TCU_ERR_ARG;
   if (!aligned16(mask) || (reinterpret_cast<uintptr_t>(count_dev) & 7u)) return TCU_ERR_ALIGN;
   if (elem_bytes != 1 && elem_bytes != 2 && elem_bytes != 4 && elem_bytes != 8) return TCU_ERR_DTYPE;
-  const int64_t tile = compress_tile(elem_bytes, idx_stage_bytes(idx_mode, idx_bytes));
+  const int64_t tile = compress_tile(elem_bytes, idx_mode, idx_bytes);
   CmpScratch sc;
   tcu_status_t s = cmp_scratch(ws, ws_bytes, n, tile, &sc);
   if (s != TCU_OK) return s;
@@ -709,7 +723,7 @@ tcu_status_t tcu_compress_counted(const void* x, int elem_bytes, const int8_t* m
   tcu_status_t s = cmp_check(x, elem_bytes, mask, idx_in, idx_bytes, idx_mode, out, idx_out);
   if (s != TCU_OK) return s;
   CmpScratch sc;
-  s = cmp_scratch(ws, ws_bytes, n, compress_tile(elem_bytes, idx_stage_bytes(idx_mode, idx_bytes)), &sc);
+  s = cmp_scratch(ws, ws_bytes, n, compress_tile(elem_bytes, idx_mode, idx_bytes), &sc);
   if (s != TCU_OK) return s;
   s = cmp_run(x, elem_bytes, mask, n, idx_in, idx_bytes, idx_mode, out, idx_out, capacity, sc, ws, st);
   if (s != TCU_OK) return s;
@@ -725,7 +739,7 @@ tcu_status_t tcu_compress(const void* x, int elem_bytes, const int8_t* mask, int
   tcu_status_t s = cmp_check(x, elem_bytes, mask, idx_in, idx_bytes, idx_mode, out, idx_out);
   if (s != TCU_OK) return s;
   if (reinterpret_cast<uintptr_t>(count_dev) & 7u) return TCU_ERR_ALIGN;
-  const int64_t tile = compress_tile(elem_bytes, idx_stage_bytes(idx_mode, idx_bytes));
+  const int64_t tile = compress_tile(elem_bytes, idx_mode, idx_bytes);
   CmpScratch sc;
   s = cmp_scratch(ws, ws_bytes, n, tile, &sc);
   if (s == TCU_OK) s = cmp_count(mask, n, tile, sc, static_cast<long long*>(count_dev), st);
@@ -747,7 +761,7 @@ tcu_status_t tcu_compress_segments(const void* x, int elem_bytes, const int8_t* 
   }
   tcu_status_t s = cmp_check(x, elem_bytes, mask, nullptr, 0, 0, out, nullptr);
   if (s != TCU_OK) return s;
-  const int64_t tile = compress_tile(elem_bytes, 0);
+  const int64_t tile = compress_tile(elem_bytes, 0, 0);
   CmpScratch sc;
   s = cmp_scratch(ws, ws_bytes, n, tile, &sc);
   if (s == TCU_OK) s = cmp_count(mask, n, tile, sc, reinterpret_cast<long long*>(seg_pos + nseg), st);
@@ -780,7 +794,7 @@ tcu_status_t tcu_split(const void* x, int elem_bytes, const int8_t* mask, int64_
   tcu_status_t s = cmp_check(x, elem_bytes, mask, idx_in, idx_bytes, idx_mode, out, idx_out);
   if (s != TCU_OK) return s;
   if (reinterpret_cast<uintptr_t>(count_dev) & 7u) return TCU_ERR_ALIGN;
-  const int64_t tile = compress_tile(elem_bytes, idx_stage_bytes(idx_mode, idx_bytes));
+  const int64_t tile = compress_tile(elem_bytes, idx_mode, idx_bytes);
   CmpScratch sc;
   s = cmp_scratch(ws, ws_bytes, n, tile, &sc);
   if (s == TCU_OK) s = cmp_count(mask, n, tile, sc, static_cast<long long*>(count_dev), st);

@@ -38,6 +38,22 @@ def test_compress_vs_oracle(dtype, n):
     assert z.dtype == x.dtype and np.array_equal(z.numpy(), ref)
 
 
+@pytest.mark.parametrize("dtype", [torch.float16, torch.int16, torch.float32, torch.int32, torch.int8, torch.float64])
+@pytest.mark.parametrize("n", [1, 17, 8191, 8192, 8193, 3 * 8192 + 77, 1_000_003])
+def test_compress_positions_vs_oracle(dtype, n):
+    """Positions of the selected elements (run_compress_ind_no_arange): the
+    compaction keeps 16-bit tile-local offsets and adds the tile start on the
+    way out, for every element size's tile length."""
+    import tcuscan_ops
+
+    x, m = _case(n, dtype, n + 5)
+    z, pos = tcuscan_ops.run_compress_ind_no_arange(x.to(DEV), m.to(DEV), 64)
+    ref = oracle.compress(x.numpy(), m.numpy())
+    want = np.nonzero(m.numpy())[0].astype(np.int32)
+    assert np.array_equal(z.cpu().numpy(), ref)
+    assert pos.dtype == torch.int32 and np.array_equal(pos.cpu().numpy(), want)
+
+
 @pytest.mark.parametrize("S", [32, 64, 128])
 @pytest.mark.parametrize("mult", [1, 3])
 @pytest.mark.parametrize("off", _OFFSETS)
