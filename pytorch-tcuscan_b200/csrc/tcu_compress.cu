@@ -71,17 +71,22 @@ struct ElemT<4> { using T = uint32_t; };
 template <>
 struct ElemT<8> { using T = unsigned long long; };
 
-// Elements per worker row for an element / index size: at most 128 bytes of
-// payload per array and row; a tile is 128 rows.
-__host__ __device__ constexpr int cmp_ept(int eb, int ib) { return eb + ib <= 2 ? 64 : (eb + ib <= 4 ? 32 : 16); }
+// Elements per worker row for an element / index size: the longest row of
+// 64, 32 or 16 elements with at most 128 bytes of each array per row (one
+// swizzled TMA box row) and a ring of at least five 128-row stages in the
+// stage budget.  An earlier rule (64 up to 2 bytes per element, 32 up to 4,
+// else 16) gave fp16 values with int32 indices 16-element rows, where 32 fit.
+__host__ __device__ constexpr int cmp_ept(int eb, int ib) {
+  return (64 * eb <= 128 && 64 * ib <= 128 && 128 * 64 * (1 + eb + ib) * 5 <= kCmpStageBudget)   ? 64
+         : (32 * eb <= 128 && 32 * ib <= 128 && 128 * 32 * (1 + eb + ib) * 5 <= kCmpStageBudget) ? 32
+                                                                                                   : 16;
+}
 // Elements per row for an index mode: gathered indices (1) are staged like
 // the values; generated positions (2) need only a 16-bit tile-local offset
-// per element in the compaction scratch, so they keep the values' row length
-// (fp16 / int8: 64, as without indices) wherever the stage ring still holds
-// five stages.  Staging 4-byte positions instead cut fp16 rows to 16
-// elements and took 620 us at 2^28 against 205 us without positions.
+// per element in the compaction scratch.  Staging 4-byte positions cut fp16
+// rows to 16 elements and took 620 us at 2^28 against 205 us without them.
 __host__ __device__ constexpr int cmp_ept_for(int eb, int idx_mode, int ib) {
-  return idx_mode == 2 ? (eb <= 2 ? 64 : (eb == 4 ? 32 : 16)) : cmp_ept(eb, idx_mode ? ib : 0);
+  return cmp_ept(eb, idx_mode == 2 ? 2 : (idx_mode ? ib : 0));
 }
 
 template <int EB, int IDX, int IB>
