@@ -172,6 +172,42 @@ __device__ __forceinline__ void vec_set(uint4* v, int j, typename ElemT<EB>::T e
   }
 }
 
+// Writes a run of `len` elements, val(0 .. len-1), to dst[g0 .. g0 + len)
+// (positions below cap only), the 128 threads of a warpgroup together:
+// 16-byte stores for the vectors that lie inside the run, element stores for
+// the ragged ends (or for all of it when dst is not 16-byte aligned).  One
+// store per element kept the store loop of split -- every element of the
+// tile written -- bound by store instructions.
+template <typename E, typename ValF>
+__device__ __forceinline__ void store_run(ValF val, int len, E* dst, long long g0, long long cap, int t) {
+  constexpr int V = 16 / (int)sizeof(E);
+  const long long end = g0 + len < cap ? g0 + len : cap;
+  if (end <= g0) return;
+  if ((reinterpret_cast<uintptr_t>(dst) & 15u) != 0) {
+    for (long long e = g0 + t; e < end; e += 128) dst[e] = val((int)(e - g0));
+    return;
+  }
+  const long long v0 = g0 / V, v1 = (end - 1) / V;
+  for (long long vb = v0 + t; vb <= v1; vb += 128) {
+    const long long e0 = vb * V;
+    if (e0 >= g0 && e0 + V <= end) {
+      union {
+        uint4 u;
+        E e[V];
+      } w;
+#pragma unroll
+      for (int i = 0; i < V; ++i) w.e[i] = val((int)(e0 - g0) + i);
+      *reinterpret_cast<uint4*>(dst + e0) = w.u;
+    } else {
+#pragma unroll
+      for (int i = 0; i < V; ++i) {
+        const long long e = e0 + i;
+        if (e >= g0 && e < end) dst[e] = val((int)(e - g0));
+      }
+    }
+  }
+}
+
 // IDX: 0 none, 1 gather idx_in (IB bytes), 2 positions (int32 when IB == 4,
 // int64 when IB == 8).  SPLIT: stable partition instead of compaction -- every
 // element is written, the selected ones at their compaction offsets and the
@@ -369,12 +405,28 @@ __global__ void __launch_bounds__(kCmpThreads, 1)
         const int valid = SPLIT ? (int)(p.n - t0 < TILE ? p.n - t0 : TILE) : total;
         // selected run at pre, unselected run after every selected element
         const long long ubase = SPLIT ? p.offsets[p.num_tiles] + (t0 - pre) - total : 0;
-        for (int i = wg_thread; i < valid; i += 128) {
-          const long long g = i < total ? pre + i : ubase + i;
-          if (g < p.capacity) {
-            static_cast<T*>(p.out)[g] = sx[i];
-            if constexpr (IDX == 1) static_cast<I*>(p.idx_out)[g] = si[i];
-            if constexpr (IDX == 2) static_cast<I*>(p.idx_out)[g] = (I)(t0 + sp[i]);
+        if constexpr (SPLIT) {
+          // every element of the tile is written: two runs with 16-byte stores
+          // (0.534 -> 0.430 ms for fp16 at 2^28); the compaction's own run
+          // (~30 % of the elements) measured no faster that way, and slower
+          // for 1-byte values, so it keeps element stores
+          T* out = static_cast<T*>(p.out);
+          I* iout = static_cast<I*>(p.idx_out);
+          const int nu = valid - total;
+          store_run<T>([&](int j) { return sx[j]; }, total, out, pre, p.capacity, wg_thread);
+          store_run<T>([&](int j) { return sx[total + j]; }, nu, out, ubase + total, p.capacity, wg_thread);
+          if constexpr (IDX == 1) {
+            store_run<I>([&](int j) { return si[j]; }, total, iout, pre, p.capacity, wg_thread);
+            store_run<I>([&](int j) { return si[total + j]; }, nu, iout, ubase + total, p.capacity, wg_thread);
+          }
+        } else {
+          for (int i = wg_thread; i < valid; i += 128) {
+            const long long g = pre + i;
+            if (g < p.capacity) {
+              static_cast<T*>(p.out)[g] = sx[i];
+              if constexpr (IDX == 1) static_cast<I*>(p.idx_out)[g] = si[i];
+              if constexpr (IDX == 2) static_cast<I*>(p.idx_out)[g] = (I)(t0 + sp[i]);
+            }
           }
         }
       }
