@@ -95,17 +95,10 @@ __device__ __forceinline__ int block_excl_scan256(int v, int* sw, int* total) {
 // its running per-digit output positions from tile to tile and no per-tile
 // offsets are stored.
 
-// Lanes of the warp whose digit equals this lane's (eight ballots).
-__device__ __forceinline__ unsigned digit_peers(int d) {
-  unsigned p = 0xffffffffu;
-#pragma unroll
-  for (int b = 0; b < 8; ++b) {
-    const bool on = (d >> b) & 1;
-    const unsigned bb = __ballot_sync(0xffffffffu, on);
-    p &= on ? bb : ~bb;
-  }
-  return p;
-}
+// Lanes of the warp whose digit equals this lane's: one match instruction
+// (eight ballots and masks per key, the earlier form, kept the scatter
+// bound by ranking instructions).
+__device__ __forceinline__ unsigned digit_peers(int d) { return __match_any_sync(0xffffffffu, d); }
 
 __host__ __device__ inline int64_t chunk_tiles(int64_t num_tiles, int chunks) {
   return (num_tiles + chunks - 1) / chunks;
